@@ -1,0 +1,134 @@
+"""Pin the CPU oracle (and the compiled reference CPU path) to the reference's known answers.
+
+Sources of the vectors: tests/golden/reference_kats.json, written by make_golden.py from
+the reference test sources (goldilocks/tests/test_helpers.hpp:17-66,
+test_ntt_cpu.cpp:182-412) and from the reference CPU build on seeded inputs.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+import oracle
+
+P = oracle.P
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<u8").tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("w", [4, 8, 12, 16])
+def test_permute_golden(orc, kats, w):
+    out = orc.permute(np.arange(w, dtype=np.uint64))
+    assert [int(v) for v in out] == kats["poseidon2"]["PERMUTE_W%d_GOLDEN" % w]
+    assert [int(v) for v in out[:4]] == kats["poseidon2"]["PERMUTE_TRUNC_W%d_GOLDEN" % w]
+
+
+@pytest.mark.parametrize("w", [8, 12, 16])
+def test_linear_hash_golden(orc, kats, w):
+    out = orc.linear_hash(w, np.arange(1, 21, dtype=np.uint64))
+    assert [int(v) for v in out] == kats["poseidon2"]["LINEAR_HASH_W%d_GOLDEN" % w]
+
+
+def test_linear_hash_empty_is_zero(orc):
+    # size 0 -> zero digest (test_poseidon2_cpu.cpp:375-389)
+    assert orc.linear_hash(16, np.zeros(0, dtype=np.uint64)).tolist() == [0, 0, 0, 0]
+
+
+def test_merkletree_reduce_golden(orc, kats):
+    root = orc.merkletree_reduce(12, np.arange(1, 13, dtype=np.uint64), 3)
+    assert [int(v) for v in root] == kats["poseidon2"]["MERKLETREE_REDUCE_W12_AR3_GOLDEN"]
+
+
+def _pmul(a, b):
+    return (a * b) % P
+
+
+def test_lde_block_golden(orc, kats):
+    # 8 columns, rows 0,1 = 1 + col, then Fibonacci; N=16 -> 32 (test_ntt_cpu.cpp:264-350)
+    n, ncols = 16, 8
+    a = [[0] * ncols for _ in range(n)]
+    for j in range(ncols):
+        a[0][j] = a[1][j] = 1 + j
+    for i in range(2, n):
+        for j in range(ncols):
+            a[i][j] = (a[i - 1][j] + a[i - 2][j]) % P
+    lde = orc.lde(np.array(a, dtype=np.uint64), 5)
+    assert [int(v) for v in lde[:, 0]] == kats["lde_block_16_32_col0"]
+
+
+def test_lde_explicit_shift49_golden(orc, kats):
+    # coefficient form with shift 49 instead of 7 (test_ntt_cpu.cpp:182-263):
+    # INTT, scale coefficient i by 49^i, zero pad, NTT on 32 points.
+    n = 16
+    a = [1, 1]
+    for i in range(2, n):
+        a.append((a[-1] + a[-2]) % P)
+    coeffs = orc.ntt(np.array(a, dtype=np.uint64).reshape(n, 1), inverse=True)[:, 0]
+    ext = np.zeros((32, 1), dtype=np.uint64)
+    g = 1
+    for i in range(n):
+        ext[i, 0] = _pmul(int(coeffs[i]), g)
+        g = _pmul(g, 49)
+    out = orc.ntt(ext)[:, 0]
+    assert [int(v) for v in out] == kats["lde_shift49_fib_16_32"]
+
+
+@pytest.mark.parametrize("case", [(16, 64, 1), (16, 32, 4), (64, 256, 8)])
+def test_lde_horner(orc, case):
+    # LDE(NTT(coeffs)) = coeffs evaluated on 7 * w_NExt^j (test_ntt_cpu.cpp:415-471)
+    n, next_, ncols = case
+    coeff = np.array([[((k * ncols + c + 1) * 1000003) % P for c in range(ncols)] for k in range(n)],
+                     dtype=np.uint64)
+    evals = orc.ntt(coeff)
+    lde = orc.lde(evals, next_.bit_length() - 1)
+    w = orc.root_of_unity(next_.bit_length() - 1)
+    wj = 1
+    for j in range(next_):
+        x = _pmul(7, wj)
+        for c in range(ncols):
+            v = int(coeff[n - 1, c])
+            for k in range(n - 2, -1, -1):
+                v = (v * x + int(coeff[k, c])) % P
+            assert int(lde[j, c]) == v
+        wj = _pmul(wj, w)
+
+
+def test_ntt_roundtrip(orc):
+    x = oracle.random_field((1 << 9, 3), 99)
+    assert (orc.ntt(orc.ntt(x), inverse=True) == x).all()
+
+
+def _seeded(kats, max_nbits):
+    return [c for c in kats["seeded_commits"] if c["nBits"] <= max_nbits]
+
+
+def test_seeded_roots_oracle(orc, kats):
+    for c in _seeded(kats, 16):
+        trace = oracle.random_field((1 << c["nBits"], c["nCols"]), c["seed"])
+        root, lde, tree = orc.commit(trace, c["nBitsExt"], c["arity"])
+        assert [int(v) for v in root] == c["root"], c
+        assert digest(lde) == c["lde_sha256"], c
+        assert digest(tree) == c["tree_sha256"], c
+
+
+def test_seeded_roots_reference_build(refcpu, kats):
+    for c in _seeded(kats, 12):
+        trace = oracle.random_field((1 << c["nBits"], c["nCols"]), c["seed"])
+        root, lde, _ = refcpu.commit(trace, c["nBitsExt"], c["arity"])
+        assert [int(v) for v in root] == c["root"], c
+
+
+def test_oracle_matches_reference_build_random(orc, refcpu):
+    for seed, (nb, nbe, nc, ar) in enumerate([(7, 8, 11, 4), (7, 9, 20, 3), (6, 7, 30, 2)]):
+        trace = oracle.random_field((1 << nb, nc), 500 + seed)
+        r1, l1, t1 = orc.commit(trace, nbe, ar)
+        r2, l2, t2 = refcpu.commit(trace, nbe, ar)
+        assert (l1 == l2).all() and (t1 == t2).all()
+
+
+def test_tree_num_elements(orc):
+    for n in [1, 2, 3, 4, 5, 16, 17, 1 << 10, (1 << 10) + 3]:
+        for ar in (2, 3, 4):
+            assert oracle.tree_num_elements(n, ar) == orc.lib.orc_tree_num_elements(n, ar)
