@@ -1,0 +1,360 @@
+#!/usr/bin/env python3
+"""Benchmark of the LDE + Poseidon2-Merkle commit (one JSON line on rank 0).
+
+Default workload: one AIR instance of 2^22 rows x 256 base columns of uniform Goldilocks
+elements, blowup 2 (LDE 2^23 rows), Poseidon2 width-16 row sponge and arity-4 tree — the
+reference's production (W16, arity 4) pairing.  A step is one full commit: row-major trace in
+HBM -> column-major LDE -> leaf digests -> every tree level -> root read back to the host.
+
+  value  GElem/s = NExt * nCols / step time, inputs resident in HBM, CUDA events on the
+         launching stream, max over ranks; every rank commits its own instance (weak scaling).
+  e2e    the same metric through the reference-compatible C ABI (commit_witness /
+         get_stream_proofs) from pinned host memory: each step copies its 8.6 GB trace to the
+         device and reads its root back; the library's two stream slots overlap one step's copy
+         with the previous step's kernels.
+
+--impl reference times the reference's own CPU implementation (NTT_Goldilocks::LDE +
+Poseidon2Goldilocks<16>::merkletree, compiled unmodified under oracle/_ref) with every host
+thread, on a bounded row sample of the same workload, in the same unit.
+"""
+import argparse
+import ctypes
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+
+WORKLOADS = {
+    "c2": dict(desc="single AIR 2^22 x 256 base columns, blowup 2, Poseidon2 W16 arity-4 tree",
+               nbits=22, nbits_ext=23, ncols=256, arity=4, sample_nbits=17),
+    "c1": dict(desc="single AIR 2^16 x 32 base columns, blowup 2, Poseidon2 W16 arity-4 tree",
+               nbits=16, nbits_ext=17, ncols=32, arity=4, sample_nbits=16),
+}
+METRIC = "LDE+Merkle commit GElem/s (NExt x nCols per second), bit-exact roots"
+UNIT = "GElem/s"
+P2_MULS = {8: 8 * 8 * 4 + 22 * (4 + 8), 12: 8 * 12 * 4 + 22 * (4 + 12), 16: 8 * 16 * 4 + 22 * (4 + 16)}
+IMAD_PER_MUL = 8  # four 32x32->64 partial products, two IMAD-pipe ops each
+
+
+def load_package():
+    name = "pil2_proofman_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    path = os.path.join(REPO, "pil2-proofman_b200", "__init__.py")
+    spec = importlib.util.spec_from_file_location(name, path, submodule_search_locations=[os.path.dirname(path)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def ncu_traffic(kernel, workload):
+    """dram read+write bytes per launch from a committed ncu summary (profiles/traffic.txt)."""
+    path = os.path.join(REPO, "profiles", "traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 3 and parts[0] == kernel and parts[1] == workload and not line.startswith("#"):
+                    return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", "b200_clocks_%d_%d.csv" % (os.getpid(), gpu_index))
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        power = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(power) if power else None}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def time_reference_cpu(wl, reps, warmup):
+    """Reference CPU LDE + tree on a row sample; returns (GElem/s, seconds per rep, threads, sample)."""
+    sys.path.insert(0, REPO)
+    import oracle  # CPU baseline leg only
+
+    threads = cpu_threads()
+    ref = oracle.RefCPU(threads=threads)
+    nb = wl["sample_nbits"]
+    b = wl["nbits_ext"] - wl["nbits"]
+    ncols, arity = wl["ncols"], wl["arity"]
+    pkg = load_package()
+    trace = pkg.fill_random_host((1 << nb) * ncols, 7).reshape(1 << nb, ncols)
+    lde = np.empty((1 << (nb + b), ncols), dtype=np.uint64)
+    tree = np.empty(oracle.tree_num_elements(1 << (nb + b), arity), dtype=np.uint64)
+    times = []
+    for i in range(warmup + reps):
+        t0 = time.perf_counter()
+        ref.lde_raw(trace, nb + b, out=lde)
+        ref.merkletree_raw(lde, arity, tree=tree)
+        t1 = time.perf_counter()
+        if i >= warmup:
+            times.append(t1 - t0)
+    sec = statistics.median(times)
+    elems = (1 << (nb + b)) * ncols
+    sample = "%d x %d trace -> %d x %d LDE + W%d arity-%d tree (1/%d of the rows), %s build" % (
+        1 << nb, ncols, 1 << (nb + b), ncols, 4 * arity, arity, 1 << (wl["nbits"] - nb), ref.variant)
+    return elems / sec / 1e9, sec, threads, sample
+
+
+def run_reference(args, wl):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    val, sec, threads, sample = time_reference_cpu(wl, args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(val, 6), "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": wl["desc"], "nBits": wl["nbits"], "nBitsExt": wl["nbits_ext"], "nCols": wl["ncols"],
+                   "arity": wl["arity"], "sample_rows": 1 << wl["sample_nbits"]},
+        "cpu_baseline": {"value": round(val, 6), "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(val, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, wl):
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    pkg = load_package()
+    pkg.init(local)
+    nbits, nbe, ncols, arity = wl["nbits"], wl["nbits_ext"], wl["ncols"], wl["arity"]
+    N, NExt = 1 << nbits, 1 << nbe
+    elems = NExt * ncols
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- resident-input path (value) -------------------------------------------------
+    stream = torch.cuda.current_stream()
+    trace = torch.empty(N * ncols, dtype=torch.int64, device=dev)
+    scratch = torch.empty(pkg.lde_scratch_words(nbits, ncols), dtype=torch.int64, device=dev)
+    lde = torch.empty(elems, dtype=torch.int64, device=dev)
+    tree = torch.empty(pkg.tree_num_elements(NExt, arity), dtype=torch.int64, device=dev)
+    pkg.fill_random_device(trace, N * ncols, 1000 + rank, stream)
+    roots = []
+    for _ in range(args.warmup):
+        roots.append(pkg.commit_device(lde, tree, trace, nbits, nbe, ncols, arity, scratch, stream=stream))
+    assert all((r == roots[0]).all() for r in roots)
+
+    pkg.timing_enable(True)
+    pkg.timing_reset()
+    launches0 = pkg.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            pkg.commit_device(lde, tree, trace, nbits, nbe, ncols, arity, scratch, stream=stream)
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = pkg.launch_count() - launches0
+    cats = pkg.timing()
+    pkg.timing_enable(False)
+    clocks = clk.summary()
+    ms = max_over_ranks(ms)
+    value = world * elems * args.steps / (ms * 1e-3) / 1e9
+
+    # ---- roofline of the dominant kernel and of the NTT passes ------------------------
+    peaks, peak_kind = measured_peaks()
+    imad = pkg.probe_imad()
+    w = 4 * arity
+    perms_per_row = max(1, -(-ncols // (w - 4)))
+    leaf_ms = cats["leaf_hash"][0] / max(1, cats["leaf_hash"][1])
+    muls = NExt * perms_per_row * P2_MULS[w]
+    achieved_gmul = muls / (leaf_ms * 1e-3) / 1e9
+    peak_gmul = imad / IMAD_PER_MUL
+    ntt_ms = sum(cats[c][0] for c in ("transpose", "ntt_inverse", "ntt_forward")) / args.steps
+    ntt_bytes = 8 * ncols * (N + NExt)
+    ntt_gbs = ntt_bytes / (ntt_ms * 1e-3) / 1e9
+    roofline = {
+        "kernel": "leaf_hash_kernel<16>",
+        "bound": "int32_imad",
+        "achieved": round(achieved_gmul, 2), "peak": round(peak_gmul, 2), "unit": "G Goldilocks-mul/s",
+        "frac": round(achieved_gmul / peak_gmul, 4),
+        "traffic": ncu_traffic("leaf_hash_kernel", args.workload),
+        "algorithmic": "%d permutations/row x %d muls (W%d) per row, %d IMAD-pipe ops per mul; peak = "
+                       "measured IMAD probe %.0f G/s / %d" % (perms_per_row, P2_MULS[w], w, IMAD_PER_MUL, imad,
+                                                             IMAD_PER_MUL),
+        "ntt": {"bound": "hbm", "achieved": round(ntt_gbs, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                "frac": round(ntt_gbs / peaks.get("hbm_gbs", 6650.0), 4),
+                "peak_kind": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind,
+                "algorithmic_bytes": "8 x nCols x (N + NExt) per commit (read trace once, write LDE once)",
+                "traffic": ncu_traffic("ntt_lde", args.workload)},
+    }
+    kernel_ms = {k: round(v[0] / args.steps, 3) for k, v in cats.items()}
+
+    # ---- end to end through the reference C ABI from pinned host memory ---------------
+    host = torch.empty(N * ncols, dtype=torch.int64, pin_memory=True)
+    host.copy_(trace)
+    del trace, scratch, lde, tree
+    torch.cuda.empty_cache()
+    lib = pkg.load()
+    pkg.set_hash_family(2)
+    bufs = pkg.DeviceBuffers(arity=arity, n_streams=2)
+    shape = pkg.StarkShape(nbits, nbe, ncols, arity)
+    params = pkg.StepsParams()
+    params.trace = host.data_ptr()
+    root_bufs = [np.zeros(4, dtype=np.uint64) for _ in range(args.warmup + args.steps)]
+    for i in range(args.warmup):
+        lib.commit_witness(shape.ptr, ctypes.addressof(params), i, 0, 0, root_bufs[i].ctypes.data, bufs.ptr, b"")
+    lib.get_stream_proofs(bufs.ptr)
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(args.warmup, args.warmup + args.steps):
+        sid = lib.commit_witness(shape.ptr, ctypes.addressof(params), i, 0, 0, root_bufs[i].ctypes.data, bufs.ptr,
+                                 b"")
+        if sid >= 2:
+            raise RuntimeError(lib.b200_last_error().decode())
+    lib.get_stream_proofs(bufs.ptr)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s)
+    if bufs.error() != 0:
+        raise RuntimeError("commit_witness failed: %s" % lib.b200_last_error().decode())
+    if not all((r == roots[0]).all() for r in root_bufs):
+        raise RuntimeError("e2e roots differ from the resident-path root")
+    e2e = world * elems * args.steps / e2e_s / 1e9
+    bufs.close()
+
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform Goldilocks)",
+        "config": {"workload": wl["desc"], "nBits": nbits, "nBitsExt": nbe, "nCols": ncols, "arity": arity,
+                   "hash": "Poseidon2 W%d" % w, "parallelism": "instance per GPU" if world > 1 else "single GPU",
+                   "l2": "inputs (%.1f GB) larger than L2; no flush" % (N * ncols * 8 / 1e9)},
+        "e2e": {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": N * ncols * 8, "d2h_bytes_per_step": 32,
+                "api": "commit_witness + get_stream_proofs, 2 stream slots, pinned host trace"},
+        "gpu_launches": int(launches),
+        "kernel_ms_per_step": kernel_ms,
+        "roofline": roofline,
+        "clocks": clocks,
+        "root": [hex(int(v)) for v in roots[0]] if rank == 0 else None,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        val, sec, threads, sample = time_reference_cpu(wl, 1, 0)
+        line["cpu_baseline"] = {"value": round(val, 6), "unit": UNIT, "cores": threads, "kind": "reference",
+                                "sample": sample}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, wl)
+    return run_ours(args, wl)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,209 @@
+/*
+ * pil2_b200 — B200-native (sm_100a) commit path for pil2-proofman:
+ * low-degree extension of Goldilocks columns + Poseidon2 Merkle tree to one root.
+ *
+ * Two groups of entry points, all extern "C", plain pointers and sizes:
+ *
+ *  1. The reference's own C ABI for the commit path, same names and signatures as
+ *     pil2-stark/src/api/starks_api.hpp, so the Rust crates (provers/starks-lib-c,
+ *     ffi_starks.rs) can bind this library in place of libstarksgpu.a.  Where the reference
+ *     passes a C++ StarkInfo/SetupCtx, this library takes the B200StarkShape below
+ *     (built with b200_stark_shape_new): the four numbers the commit reads.
+ *
+ *  2. A native API on device or host buffers (prefix b200_), used by the tests and the
+ *     benchmark, and by callers that manage device memory themselves.
+ *
+ * Conventions
+ *  - Field elements are uint64_t; results are canonical (x mod p, p = 2^64 - 2^32 + 1);
+ *    inputs may be any 64-bit value (taken mod p).
+ *  - Device LDE buffers are column-major: element (row, col) at col*NExt + row
+ *    (the reference GPU layout, goldilocks_trace_layout.cuh:14-46).  Traces given as
+ *    row-major are element (row, col) at row*nCols + col (the reference CPU layout).
+ *  - Tree buffers have b200_tree_num_elements(rows, arity) words in the reference layout
+ *    (poseidon2_goldilocks.cpp:129-175); the root is the last 4 words.
+ *  - Arity 2, 3, 4 uses Poseidon2 width 8, 12, 16 (merkleTreeGL.cpp:316-336).
+ *  - int-returning functions return 0 on success and a negative B200_E* code on error;
+ *    b200_last_error() describes the last error of the calling thread.  No entry point
+ *    aborts the process.
+ */
+#ifndef PIL2_B200_H
+#define PIL2_B200_H
+
+#include <stdbool.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B200_OK 0
+#define B200_EINVAL -1    /* bad shape / argument */
+#define B200_ECUDA -2     /* CUDA runtime error */
+#define B200_ENOMEM -3    /* device or host allocation failed */
+#define B200_EFAMILY -4   /* hash family not set, or not Poseidon2 */
+#define B200_EBUSY -5     /* no admission (serving queue full / budget) */
+#define B200_ETIMEOUT -6  /* bounded wait expired */
+
+/* ------------------------------------------------------------------------------------
+ * 1. Reference C ABI (pil2-stark/src/api/starks_api.hpp)
+ * ------------------------------------------------------------------------------------ */
+
+/* Shape descriptor standing in for StarkInfo / SetupCtx: nBits, nBitsExt, the committed
+ * column count (mapSectionsN["cm1"] for commit_witness, nConstants for
+ * calculate_const_tree) and merkleTreeArity (stark_info.cpp:24-60). */
+typedef struct B200StarkShape {
+    uint64_t nBits;
+    uint64_t nBitsExt;
+    uint64_t nCols;
+    uint64_t arity;
+} B200StarkShape;
+
+/* Layout of StepsParams (starkpil/steps.hpp:6-20 == common/src/air_instance.rs:20-33);
+ * commit_witness reads `trace` (host, row-major N x nCols). */
+typedef struct B200StepsParams {
+    uint64_t *trace;
+    uint64_t *aux_trace;
+    uint64_t *publicInputs;
+    uint64_t *proofValues;
+    uint64_t *challenges;
+    uint64_t *airgroupValues;
+    uint64_t *airValues;
+    uint64_t *evals;
+    uint64_t *xDivXSub;
+    uint64_t *pConstPolsAddress;
+    uint64_t *pConstPolsExtendedTreeAddress;
+    uint64_t *pCustomCommitsFixed;
+} B200StepsParams;
+
+/* starks_api.hpp:28 — 1 = Poseidon1 (not provided: later commits fail with B200_EFAMILY),
+ * 2 = Poseidon2.  Must be called before the reference-ABI commit entries. */
+void set_hash_family(uint8_t fam);
+
+/* starks_api.hpp:52 — per-device set-up (twiddle/coset tables, kernel attributes) for the
+ * current device.  The Poseidon2 constants are compiled in. */
+void init_gpu_setup(uint64_t arity);
+
+/* starks_api.hpp:190,193 — device commit buffers: a pool of streams, each owning device
+ * buffers for one commit (grown on demand, kept resident until the slot is reused so the
+ * LDE and tree can be read by later queries).  node_rank/node_size/numa_nodes are accepted
+ * for signature compatibility; this library uses the current device. */
+void *gen_device_buffers(uint32_t node_rank, uint32_t node_size, const int32_t *numa_nodes, uint32_t arity,
+                         uint32_t max_n_bits_ext);
+void free_device_buffers(void *d_buffers);
+
+/* starks_api.hpp:198 — resize the stream pool to n_streams slots (other args accepted for
+ * signature compatibility).  Returns the number of slots. */
+uint64_t gen_device_streams(void *d_buffers, uint64_t n_streams, uint64_t n_recursive_streams,
+                            const uint64_t *auxTraceSizes, uint64_t maxSizeProverBufferAggregation,
+                            uint64_t maxProofSize, uint64_t merkleTreeArity);
+
+/* starks_api.hpp:96 — synchronous: LDE + tree of a row-major host buffer N x nCols; writes the
+ * 4-word root.  If bufferFile is a non-empty path, writes [root 32 B][source N*nCols words]
+ * [LDE NExt*nCols words][tree nodes] with source and LDE column-major, as the reference's GPU
+ * backend does (starks_api.cu:1867-1930). */
+void write_custom_commit(void *root, uint64_t arity, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols,
+                         void *d_buffers, void *buffer, char *bufferFile);
+
+/* starks_api.hpp:98 — asynchronous stage-1 commit of params->trace (host, row-major).
+ * pSetupCtx is a B200StarkShape*.  Returns the stream slot id (or UINT64_MAX on error); the
+ * root is written to `root` when get_stream_proofs / get_stream_proofs_non_blocking harvests
+ * the slot.  The host trace may be reused after wait_trace_h2d_done(d_buffers, slot). */
+uint64_t commit_witness(void *pSetupCtx, void *params, uint64_t instanceId, uint64_t airgroupId, uint64_t airId,
+                        void *root, void *d_buffers, char *customCommitsFixedPath);
+
+/* starks_api.hpp:127-128 — harvest finished commits (blocking: all in flight). */
+void get_stream_proofs(void *d_buffers);
+void get_stream_proofs_non_blocking(void *d_buffers);
+
+/* starks_api.hpp:42 */
+void wait_trace_h2d_done(void *d_buffers, uint64_t stream_id);
+
+/* starks_api.hpp:61 — pStarkInfo is a B200StarkShape* (nCols = nConstants).  Host const pols
+ * N x nConstants row-major in, host tree out: [LDE column-major NExt*nConstants][nodes]
+ * (calculate_const_tree_gpu, starks_api.cu:1932-1980).  unified_buffer_gpu, if non-NULL, is a
+ * device buffer of at least that many words used instead of a temporary allocation. */
+void calculate_const_tree(void *pStarkInfo, void *pConstPolsAddress, void *pConstTree, void *unified_buffer_gpu);
+
+/* starks_api.hpp:58 — words in the const tree buffer above */
+uint64_t get_const_tree_size(void *pStarkInfo);
+
+/* starks_api.hpp:230 — this library is GPU-only: returns true, ignores false */
+bool set_gpu_mode(bool use_gpu);
+
+/* ------------------------------------------------------------------------------------
+ * 2. Native API
+ * ------------------------------------------------------------------------------------ */
+
+void *b200_stark_shape_new(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t arity);
+void b200_stark_shape_free(void *shape);
+
+const char *b200_last_error(void);
+/* last error recorded on a d_buffers object by a void reference-ABI call (0 if none) */
+int b200_buffers_error(void *d_buffers);
+
+/* sets up the given device (tables, attributes); called implicitly by every entry point */
+int b200_init(int device);
+int b200_device_count(void);
+
+uint64_t b200_tree_num_elements(uint64_t nrows, uint64_t arity);
+/* words of scratch the LDE needs (one column-major copy of the trace) */
+uint64_t b200_lde_scratch_words(uint64_t nBits, uint64_t nCols);
+
+/* Device-pointer API; stream is a cudaStream_t (NULL = legacy default stream).  All calls
+ * are asynchronous on `stream` except where a host output is requested. */
+
+/* LDE: d_lde column-major NExt x nCols; d_trace row-major (trace_rowmajor != 0) or column-major
+ * with stride N; d_scratch holds b200_lde_scratch_words() words and overlaps neither. */
+int b200_lde_device(uint64_t *d_lde, const uint64_t *d_trace, int trace_rowmajor, uint64_t nBits,
+                    uint64_t nBitsExt, uint64_t nCols, uint64_t *d_scratch, void *stream);
+
+/* Merkle tree (leaf sponge + levels) over element (row, col) = d_src[row*rs + col*cs]. */
+int b200_merkletree_device(uint64_t *d_tree, const uint64_t *d_src, uint64_t rs, uint64_t cs, uint64_t nCols,
+                           uint64_t nRows, uint64_t arity, void *stream);
+
+/* LDE + tree.  If root_host is non-NULL, the root is copied there and the stream synchronised. */
+int b200_commit_device(uint64_t *root_host, uint64_t *d_lde, uint64_t *d_tree, const uint64_t *d_trace,
+                       int trace_rowmajor, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t arity,
+                       uint64_t *d_scratch, void *stream);
+
+/* n independent Poseidon2 permutations of width 8/12/16 (d_in, d_out: n*width words). */
+int b200_permute_device(uint64_t *d_out, const uint64_t *d_in, uint64_t n, uint64_t width, void *stream);
+
+/* Host-buffer API (synchronous, allocates its own device memory): row-major trace in,
+ * root out; lde_out (column-major NExt x nCols) and tree_out may be NULL. */
+int b200_commit_host(uint64_t *root, uint64_t *lde_out, uint64_t *tree_out, const uint64_t *trace, uint64_t nBits,
+                     uint64_t nBitsExt, uint64_t nCols, uint64_t arity);
+
+/* Seeded synthetic field data: element i = the first splitmix64 output below p from the
+ * stream keyed by (seed, i).  Host and device versions give identical values. */
+int b200_fill_random_device(uint64_t *d_buf, uint64_t n, uint64_t seed, void *stream);
+void b200_fill_random_host(uint64_t *buf, uint64_t n, uint64_t seed);
+
+/* Rows of a resident LDE (query openings): out[i*nCols + c] = lde[c*NExt + rows[i]]. */
+int b200_lde_rows_device(uint64_t *d_out, const uint64_t *d_lde, uint64_t NExt, uint64_t nCols,
+                         const uint64_t *d_rows, uint64_t nrows_req, void *stream);
+
+/* Names of the kernels this library launches (for test evidence), newline separated. */
+const char *b200_kernel_names(void);
+
+/* Kernel-category GPU timers (cudaEvent pairs on the launching stream; off by default).
+ * Categories: 0 transpose, 1 ntt_inverse, 2 ntt_forward, 3 leaf_hash, 4 tree_levels.
+ * b200_timing_get waits for the recorded events and returns the category's total ms and
+ * the number of timed launch groups. */
+void b200_timing_enable(int on);
+void b200_timing_reset(void);
+int b200_timing_get(int category, double *total_ms, uint64_t *count);
+const char *b200_timing_name(int category);
+
+/* Kernels launched by this library since the process started. */
+uint64_t b200_launch_count(void);
+
+/* INT32 multiply-add throughput probe: `blocks` x 256 threads each run 8 independent
+ * mad.lo/mad.hi chains of `iters` steps; returns the measured rate in G IMAD/s. */
+int b200_probe_imad(uint64_t blocks, uint64_t iters, double *gimad_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PIL2_B200_H */

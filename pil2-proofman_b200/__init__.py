@@ -1,0 +1,282 @@
+"""Python host mirror of the pil2_b200 C ABI (include/pil2_b200.h).
+
+The product is the CUDA shared library ``libpil2_b200.so`` built from ``csrc/`` for
+sm_100a; this module only binds it with ctypes, mirroring the reference's commit
+entry points (pil2-stark/src/api/starks_api.hpp) and the native ``b200_*`` API.
+There is no CPU fallback: if the library is missing or no GPU is present, calls fail.
+
+Device buffers are passed as raw pointers; torch tensors (dtype int64 or uint64,
+used only as 64-bit storage) are accepted wherever a device pointer is expected.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpil2_b200.so")
+P = 0xFFFFFFFF00000001
+
+B200_OK = 0
+B200_EINVAL = -1
+B200_ECUDA = -2
+B200_ENOMEM = -3
+B200_EFAMILY = -4
+B200_EBUSY = -5
+B200_ETIMEOUT = -6
+
+_u64 = ctypes.c_uint64
+_i32 = ctypes.c_int
+_vp = ctypes.c_void_p
+_pu64 = ctypes.POINTER(ctypes.c_uint64)
+
+_SIGS = {
+    # reference ABI
+    "set_hash_family": (None, [ctypes.c_uint8]),
+    "init_gpu_setup": (None, [_u64]),
+    "gen_device_buffers": (_vp, [ctypes.c_uint32, ctypes.c_uint32, _vp, ctypes.c_uint32, ctypes.c_uint32]),
+    "free_device_buffers": (None, [_vp]),
+    "gen_device_streams": (_u64, [_vp, _u64, _u64, _vp, _u64, _u64, _u64]),
+    "write_custom_commit": (None, [_vp, _u64, _u64, _u64, _u64, _vp, _vp, ctypes.c_char_p]),
+    "commit_witness": (_u64, [_vp, _vp, _u64, _u64, _u64, _vp, _vp, ctypes.c_char_p]),
+    "get_stream_proofs": (None, [_vp]),
+    "get_stream_proofs_non_blocking": (None, [_vp]),
+    "wait_trace_h2d_done": (None, [_vp, _u64]),
+    "calculate_const_tree": (None, [_vp, _vp, _vp, _vp]),
+    "get_const_tree_size": (_u64, [_vp]),
+    "set_gpu_mode": (ctypes.c_bool, [ctypes.c_bool]),
+    # native
+    "b200_stark_shape_new": (_vp, [_u64, _u64, _u64, _u64]),
+    "b200_stark_shape_free": (None, [_vp]),
+    "b200_last_error": (ctypes.c_char_p, []),
+    "b200_buffers_error": (_i32, [_vp]),
+    "b200_init": (_i32, [_i32]),
+    "b200_device_count": (_i32, []),
+    "b200_tree_num_elements": (_u64, [_u64, _u64]),
+    "b200_lde_scratch_words": (_u64, [_u64, _u64]),
+    "b200_lde_device": (_i32, [_vp, _vp, _i32, _u64, _u64, _u64, _vp, _vp]),
+    "b200_merkletree_device": (_i32, [_vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp]),
+    "b200_commit_device": (_i32, [_vp, _vp, _vp, _vp, _i32, _u64, _u64, _u64, _u64, _vp, _vp]),
+    "b200_permute_device": (_i32, [_vp, _vp, _u64, _u64, _vp]),
+    "b200_commit_host": (_i32, [_vp, _vp, _vp, _vp, _u64, _u64, _u64, _u64]),
+    "b200_fill_random_device": (_i32, [_vp, _u64, _u64, _vp]),
+    "b200_fill_random_host": (None, [_vp, _u64, _u64]),
+    "b200_lde_rows_device": (_i32, [_vp, _vp, _u64, _u64, _vp, _u64, _vp]),
+    "b200_kernel_names": (ctypes.c_char_p, []),
+    "b200_timing_enable": (None, [_i32]),
+    "b200_timing_reset": (None, []),
+    "b200_timing_get": (_i32, [_i32, ctypes.POINTER(ctypes.c_double), _pu64]),
+    "b200_timing_name": (ctypes.c_char_p, [_i32]),
+    "b200_launch_count": (_u64, []),
+    "b200_probe_imad": (_i32, [_u64, _u64, ctypes.POINTER(ctypes.c_double)]),
+}
+
+_lib = None
+
+
+def load(path=LIB_PATH):
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError("%s is missing: build it with `python %s`" % (path, os.path.join(HERE, "build.py")))
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in _SIGS.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+class B200Error(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("pil2_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+def _check(rc):
+    if rc != 0:
+        raise B200Error(rc, (load().b200_last_error() or b"").decode())
+    return rc
+
+
+def _ptr(x):
+    """Device/host pointer of a torch tensor, numpy array, int or None."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if isinstance(x, np.ndarray):
+        assert x.dtype == np.uint64 and x.flags["C_CONTIGUOUS"]
+        return x.ctypes.data
+    # torch tensor
+    assert x.element_size() == 8 and x.is_contiguous()
+    return x.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream  # torch.cuda.Stream
+
+
+def tree_num_elements(nrows, arity):
+    return int(load().b200_tree_num_elements(nrows, arity))
+
+
+def lde_scratch_words(nbits, ncols):
+    return int(load().b200_lde_scratch_words(nbits, ncols))
+
+
+def init(device=0):
+    _check(load().b200_init(device))
+
+
+# ---------------------------------------------------------------- native API ----
+
+def lde_device(d_lde, d_trace, nbits, nbits_ext, ncols, d_scratch, trace_rowmajor=True, stream=None):
+    _check(load().b200_lde_device(_ptr(d_lde), _ptr(d_trace), 1 if trace_rowmajor else 0, nbits, nbits_ext,
+                                  ncols, _ptr(d_scratch), _stream(stream)))
+
+
+def merkletree_device(d_tree, d_src, rs, cs, ncols, nrows, arity, stream=None):
+    _check(load().b200_merkletree_device(_ptr(d_tree), _ptr(d_src), rs, cs, ncols, nrows, arity, _stream(stream)))
+
+
+def commit_device(d_lde, d_tree, d_trace, nbits, nbits_ext, ncols, arity, d_scratch, trace_rowmajor=True,
+                  stream=None, want_root=True):
+    root = np.zeros(4, dtype=np.uint64) if want_root else None
+    _check(load().b200_commit_device(_ptr(root), _ptr(d_lde), _ptr(d_tree), _ptr(d_trace),
+                                     1 if trace_rowmajor else 0, nbits, nbits_ext, ncols, arity, _ptr(d_scratch),
+                                     _stream(stream)))
+    return root
+
+
+def permute_device(d_out, d_in, n, width, stream=None):
+    _check(load().b200_permute_device(_ptr(d_out), _ptr(d_in), n, width, _stream(stream)))
+
+
+def fill_random_device(d_buf, n, seed, stream=None):
+    _check(load().b200_fill_random_device(_ptr(d_buf), n, seed, _stream(stream)))
+
+
+def fill_random_host(n, seed):
+    out = np.empty(n, dtype=np.uint64)
+    load().b200_fill_random_host(_ptr(out), n, seed)
+    return out
+
+
+def lde_rows_device(d_out, d_lde, next_, ncols, d_rows, nreq, stream=None):
+    _check(load().b200_lde_rows_device(_ptr(d_out), _ptr(d_lde), next_, ncols, _ptr(d_rows), nreq, _stream(stream)))
+
+
+def commit_host(trace, nbits_ext, arity, want_lde=False, want_tree=False):
+    """Row-major (N, nCols) uint64 trace -> (root[4], lde column-major (nCols, NExt) or None, tree or None)."""
+    trace = np.ascontiguousarray(trace, dtype=np.uint64)
+    n, ncols = trace.shape
+    nbits = n.bit_length() - 1
+    assert 1 << nbits == n
+    next_ = 1 << nbits_ext
+    root = np.zeros(4, dtype=np.uint64)
+    lde = np.zeros((ncols, next_), dtype=np.uint64) if want_lde else None
+    tree = np.zeros(tree_num_elements(next_, arity), dtype=np.uint64) if want_tree else None
+    _check(load().b200_commit_host(_ptr(root), _ptr(lde), _ptr(tree), _ptr(trace), nbits, nbits_ext, ncols, arity))
+    return root, lde, tree
+
+
+def kernel_names():
+    return load().b200_kernel_names().decode().split()
+
+
+# ------------------------------------------------------------ reference ABI ----
+
+class StepsParams(ctypes.Structure):
+    """starkpil/steps.hpp:6-20 — twelve pointers; commit_witness reads `trace`."""
+    _fields_ = [(n, ctypes.c_void_p) for n in (
+        "trace", "aux_trace", "publicInputs", "proofValues", "challenges", "airgroupValues", "airValues",
+        "evals", "xDivXSub", "pConstPolsAddress", "pConstPolsExtendedTreeAddress", "pCustomCommitsFixed")]
+
+
+class StarkShape:
+    """Owns a B200StarkShape (stands in for StarkInfo / SetupCtx on the commit path)."""
+
+    def __init__(self, nbits, nbits_ext, ncols, arity):
+        self.ptr = load().b200_stark_shape_new(nbits, nbits_ext, ncols, arity)
+        self.nbits, self.nbits_ext, self.ncols, self.arity = nbits, nbits_ext, ncols, arity
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and _lib is not None:
+            _lib.b200_stark_shape_free(self.ptr)
+            self.ptr = None
+
+
+class DeviceBuffers:
+    """gen_device_buffers / free_device_buffers (starks_api.hpp:190,193)."""
+
+    def __init__(self, arity=4, max_n_bits_ext=0, n_streams=2):
+        lib = load()
+        self.ptr = lib.gen_device_buffers(0, 1, None, arity, max_n_bits_ext)
+        if not self.ptr:
+            raise B200Error(B200_ENOMEM, (lib.b200_last_error() or b"").decode())
+        if n_streams != 2:
+            lib.gen_device_streams(self.ptr, n_streams, 0, None, 0, 0, arity)
+
+    def error(self):
+        return int(load().b200_buffers_error(self.ptr))
+
+    def close(self):
+        if self.ptr:
+            load().free_device_buffers(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        if _lib is not None:
+            self.close()
+
+
+def set_hash_family(fam):
+    load().set_hash_family(fam)
+
+
+# ----------------------------------------------------------------- profiling ----
+
+TIMING_CATEGORIES = ("transpose", "ntt_inverse", "ntt_forward", "leaf_hash", "tree_levels")
+
+
+def timing_enable(on=True):
+    load().b200_timing_enable(1 if on else 0)
+
+
+def timing_reset():
+    load().b200_timing_reset()
+
+
+def timing():
+    """{category: (total_ms, launch_groups)} since the last reset (waits for the events)."""
+    lib = load()
+    out = {}
+    for i, name in enumerate(TIMING_CATEGORIES):
+        ms = ctypes.c_double()
+        cnt = ctypes.c_uint64()
+        _check(lib.b200_timing_get(i, ctypes.byref(ms), ctypes.byref(cnt)))
+        out[name] = (ms.value, cnt.value)
+    return out
+
+
+def launch_count():
+    return int(load().b200_launch_count())
+
+
+def probe_imad(blocks=148 * 16, iters=1 << 16):
+    r = ctypes.c_double()
+    _check(load().b200_probe_imad(blocks, iters, ctypes.byref(r)))
+    return r.value
+

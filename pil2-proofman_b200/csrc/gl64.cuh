@@ -1,0 +1,256 @@
+// Goldilocks field GF(p), p = 2^64 - 2^32 + 1, for sm_100a.
+//
+// Elements are plain uint64_t.  Device arithmetic keeps them "loose": any value in
+// [0, 2^64) stands for itself mod p, the way the reference's GPU build keeps them
+// partially reduced (GL64_PARTIALLY_REDUCED, goldilocks/Makefile:134).  Canonical
+// form (x mod p) is produced only where values leave the library (gl_canon).
+//
+// The 64x64 product is formed from 32-bit IMAD/IMAD.HI carry chains and reduced
+// with 2^64 = 2^32 - 1 and 2^96 = -1 (mod p); no 64-bit multiply is used.
+// Reference semantics: goldilocks_base_field_scalar.hpp:16-41 (add/sub), :229-258 (mul).
+#pragma once
+#include <stdint.h>
+
+#define GL_P 0xFFFFFFFF00000001ULL
+#define GL_EPS 0x00000000FFFFFFFFULL  // 2^64 mod p
+
+namespace gl {
+
+__device__ __forceinline__ uint32_t lo32(uint64_t x) { return (uint32_t)x; }
+__device__ __forceinline__ uint32_t hi32(uint64_t x) { return (uint32_t)(x >> 32); }
+__device__ __forceinline__ uint64_t mk64(uint32_t lo, uint32_t hi) { return ((uint64_t)hi << 32) | lo; }
+
+// canonical representative
+__device__ __forceinline__ uint64_t canon(uint64_t a) { return a >= GL_P ? a - GL_P : a; }
+
+// Reduce the 128-bit value (r3:r2:r1:r0) to a loose 64-bit representative:
+//   x = lo + hl*2^64 + hh*2^96 = lo + hl*(2^32-1) - hh  (mod p),
+// where lo = r1:r0, hl = r2, hh = r3.  The signed carry c in {-1,0,1} of that sum is
+// folded back as c*(2^32-1) (two's complement: +EPS or +p), which cannot wrap again.
+__device__ __forceinline__ uint64_t reduce128(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3)
+{
+    uint32_t z0, z1, c, t0, t1;
+    asm("mad.lo.cc.u32  %0, %5, 0xffffffff, %3;\n\t"
+        "madc.hi.cc.u32 %1, %5, 0xffffffff, %4;\n\t"
+        "addc.u32       %2, 0, 0;\n\t"
+        "sub.cc.u32     %0, %0, %6;\n\t"
+        "subc.cc.u32    %1, %1, 0;\n\t"
+        "subc.u32       %2, %2, 0;\n\t"
+        : "=r"(z0), "=r"(z1), "=r"(c)
+        : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
+    t0 = 0u - c;                    // c=1 -> 0xffffffff, c=-1 -> 1, c=0 -> 0
+    t1 = (uint32_t)((int32_t)c >> 31);  // c=-1 -> 0xffffffff
+    asm("add.cc.u32 %0, %0, %2;\n\t"
+        "addc.u32   %1, %1, %3;\n\t"
+        : "+r"(z0), "+r"(z1)
+        : "r"(t0), "r"(t1));
+    return mk64(z0, z1);
+}
+
+// full 128-bit product of two 64-bit values, (r3:r2:r1:r0)
+__device__ __forceinline__ void mul128(uint64_t a, uint64_t b, uint32_t &r0, uint32_t &r1, uint32_t &r2,
+                                       uint32_t &r3)
+{
+    uint32_t a0 = lo32(a), a1 = hi32(a), b0 = lo32(b), b1 = hi32(b);
+    asm("mul.lo.u32     %0, %4, %6;\n\t"
+        "mul.hi.u32     %1, %4, %6;\n\t"
+        "mad.lo.cc.u32  %1, %4, %7, %1;\n\t"
+        "madc.hi.u32    %2, %4, %7, 0;\n\t"
+        "mad.lo.cc.u32  %1, %5, %6, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+        "madc.hi.u32    %3, %5, %7, 0;\n\t"
+        "mad.lo.cc.u32  %2, %5, %7, %2;\n\t"
+        "addc.u32       %3, %3, 0;\n\t"
+        : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+        : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b)
+{
+    uint32_t r0, r1, r2, r3;
+    mul128(a, b, r0, r1, r2, r3);
+    return reduce128(r0, r1, r2, r3);
+}
+
+// a*b + c as one 128-bit value, one reduction ((2^64-1)^2 + 2^64-1 < 2^128)
+__device__ __forceinline__ uint64_t mul_add(uint64_t a, uint64_t b, uint64_t c)
+{
+    uint32_t r0, r1, r2, r3;
+    mul128(a, b, r0, r1, r2, r3);
+    asm("add.cc.u32  %0, %0, %4;\n\t"
+        "addc.cc.u32 %1, %1, %5;\n\t"
+        "addc.cc.u32 %2, %2, 0;\n\t"
+        "addc.u32    %3, %3, 0;\n\t"
+        : "+r"(r0), "+r"(r1), "+r"(r2), "+r"(r3)
+        : "r"(lo32(c)), "r"(hi32(c)));
+    return reduce128(r0, r1, r2, r3);
+}
+
+__device__ __forceinline__ uint64_t sqr(uint64_t a) { return mul(a, a); }
+
+// a + b for loose a and loose b: a carry out of 2^64 is worth EPS; a second carry
+// (both operands near 2^64) is folded the same way and cannot repeat.
+__device__ __forceinline__ uint64_t add(uint64_t a, uint64_t b)
+{
+    uint32_t s0, s1, c;
+    asm("add.cc.u32  %0, %3, %5;\n\t"
+        "addc.cc.u32 %1, %4, %6;\n\t"
+        "addc.u32    %2, 0, 0;\n\t"
+        : "=r"(s0), "=r"(s1), "=r"(c)
+        : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
+    uint32_t m = 0u - c;
+    asm("add.cc.u32  %0, %0, %3;\n\t"
+        "addc.cc.u32 %1, %1, 0;\n\t"
+        "addc.u32    %2, 0, 0;\n\t"
+        : "+r"(s0), "+r"(s1), "=r"(c)
+        : "r"(m));
+    m = 0u - c;
+    asm("add.cc.u32  %0, %0, %2;\n\t"
+        "addc.u32    %1, %1, 0;\n\t"
+        : "+r"(s0), "+r"(s1)
+        : "r"(m));
+    return mk64(s0, s1);
+}
+
+// a + b where b < p (canonical): at most one carry fix-up is needed
+__device__ __forceinline__ uint64_t add_c(uint64_t a, uint64_t b)
+{
+    uint32_t s0, s1, c;
+    asm("add.cc.u32  %0, %3, %5;\n\t"
+        "addc.cc.u32 %1, %4, %6;\n\t"
+        "addc.u32    %2, 0, 0;\n\t"
+        : "=r"(s0), "=r"(s1), "=r"(c)
+        : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
+    uint32_t m = 0u - c;
+    asm("add.cc.u32  %0, %0, %2;\n\t"
+        "addc.u32    %1, %1, 0;\n\t"
+        : "+r"(s0), "+r"(s1)
+        : "r"(m));
+    return mk64(s0, s1);
+}
+
+// a - b for loose a, b: a borrow is worth -EPS; a second borrow is folded the same way.
+__device__ __forceinline__ uint64_t sub(uint64_t a, uint64_t b)
+{
+    uint32_t s0, s1, c;
+    asm("sub.cc.u32  %0, %3, %5;\n\t"
+        "subc.cc.u32 %1, %4, %6;\n\t"
+        "subc.u32    %2, 0, 0;\n\t"
+        : "=r"(s0), "=r"(s1), "=r"(c)
+        : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
+    uint32_t m = c;  // 0 or 0xffffffff (= EPS low word)
+    asm("sub.cc.u32  %0, %0, %3;\n\t"
+        "subc.cc.u32 %1, %1, 0;\n\t"
+        "subc.u32    %2, 0, 0;\n\t"
+        : "+r"(s0), "+r"(s1), "=r"(c)
+        : "r"(m));
+    m = c;
+    asm("sub.cc.u32  %0, %0, %2;\n\t"
+        "subc.u32    %1, %1, 0;\n\t"
+        : "+r"(s0), "+r"(s1)
+        : "r"(m));
+    return mk64(s0, s1);
+}
+
+// x^7 = x^3 * x^4, the Poseidon2 S-box (poseidon2_goldilocks.hpp:147-155)
+__device__ __forceinline__ uint64_t pow7(uint64_t x)
+{
+    uint64_t x2 = sqr(x);
+    uint64_t x3 = mul(x, x2);
+    uint64_t x4 = sqr(x2);
+    return mul(x3, x4);
+}
+
+// ---- 96-bit accumulators for linear layers with small positive coefficients ----
+struct Acc {
+    uint32_t w0, w1, w2;
+};
+
+__device__ __forceinline__ Acc acc(uint64_t a) { return Acc{lo32(a), hi32(a), 0u}; }
+
+__device__ __forceinline__ Acc acc_add(Acc a, Acc b)
+{
+    Acc r;
+    asm("add.cc.u32  %0, %3, %6;\n\t"
+        "addc.cc.u32 %1, %4, %7;\n\t"
+        "addc.u32    %2, %5, %8;\n\t"
+        : "=r"(r.w0), "=r"(r.w1), "=r"(r.w2)
+        : "r"(a.w0), "r"(a.w1), "r"(a.w2), "r"(b.w0), "r"(b.w1), "r"(b.w2));
+    return r;
+}
+
+__device__ __forceinline__ Acc acc_add64(Acc a, uint64_t b)
+{
+    Acc r;
+    asm("add.cc.u32  %0, %3, %5;\n\t"
+        "addc.cc.u32 %1, %4, %6;\n\t"
+        "addc.u32    %2, %7, 0;\n\t"
+        : "=r"(r.w0), "=r"(r.w1), "=r"(r.w2)
+        : "r"(a.w0), "r"(a.w1), "r"(lo32(b)), "r"(hi32(b)), "r"(a.w2));
+    return r;
+}
+
+__device__ __forceinline__ Acc acc_add6464(uint64_t a, uint64_t b)
+{
+    Acc r;
+    asm("add.cc.u32  %0, %3, %5;\n\t"
+        "addc.cc.u32 %1, %4, %6;\n\t"
+        "addc.u32    %2, 0, 0;\n\t"
+        : "=r"(r.w0), "=r"(r.w1), "=r"(r.w2)
+        : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
+    return r;
+}
+
+// fold (w2:w1:w0) = lo + w2*2^64 = lo + w2*(2^32-1): a single carry may remain, worth EPS
+__device__ __forceinline__ uint64_t acc_reduce(Acc a)
+{
+    uint32_t z0, z1, c;
+    asm("mad.lo.cc.u32  %0, %5, 0xffffffff, %3;\n\t"
+        "madc.hi.cc.u32 %1, %5, 0xffffffff, %4;\n\t"
+        "addc.u32       %2, 0, 0;\n\t"
+        : "=r"(z0), "=r"(z1), "=r"(c)
+        : "r"(a.w0), "r"(a.w1), "r"(a.w2));
+    uint32_t m = 0u - c;
+    asm("add.cc.u32  %0, %0, %2;\n\t"
+        "addc.u32    %1, %1, 0;\n\t"
+        : "+r"(z0), "+r"(z1)
+        : "r"(m));
+    return mk64(z0, z1);
+}
+
+}  // namespace gl
+
+// ---------------------------------------------------------------- host side ----
+namespace glh {
+static inline uint64_t canon(uint64_t a) { return a >= GL_P ? a - GL_P : a; }
+static inline uint64_t mul(uint64_t a, uint64_t b)
+{
+    unsigned __int128 x = (unsigned __int128)a * b;
+    return (uint64_t)(x % GL_P);
+}
+static inline uint64_t add(uint64_t a, uint64_t b)
+{
+    unsigned __int128 x = (unsigned __int128)a + b;
+    return (uint64_t)(x % GL_P);
+}
+static inline uint64_t pow(uint64_t b, uint64_t e)
+{
+    uint64_t acc = 1;
+    b = canon(b);
+    while (e) {
+        if (e & 1) acc = mul(acc, b);
+        b = mul(b, b);
+        e >>= 1;
+    }
+    return acc;
+}
+static inline uint64_t inv(uint64_t a) { return pow(a, GL_P - 2); }
+// W[k]: the reference's 2^k-th roots of unity (goldilocks_base_field.cpp:11-44), which are
+// W[32] = 0x64fdd1a46201e246 squared down: W[k] = W[k+1]^2.
+static inline uint64_t root_of_unity(unsigned k)
+{
+    uint64_t w = 0x64fdd1a46201e246ULL;
+    for (unsigned i = 32; i > k; i--) w = mul(w, w);
+    return w;
+}
+}  // namespace glh

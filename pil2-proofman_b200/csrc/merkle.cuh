@@ -1,0 +1,155 @@
+// Poseidon2 row sponge ("linear hash") and arity-k Merkle tree levels.
+//
+// Semantics follow the reference CPU path bit for bit:
+//   linear hash  poseidon2_goldilocks.cpp:42-77 — capacity zeroed at the start; every
+//                block overwrites words [0, n) with input, zero-fills [n, RATE) and carries
+//                the previous output words [0, 4) into the capacity; no length padding;
+//                0 columns give the zero digest.
+//   tree         poseidon2_goldilocks.cpp:129-175 — digests of a level are contiguous
+//                4-word groups; (arity - pending % arity) % arity zero digests pad the level
+//                inside the buffer; parent i is the first 4 words of the permutation of the
+//                W = 4*arity words of its children; the root is the last 4 words
+//                (goldilocks_tooling.hpp:9-21 gives the buffer size).
+//
+// Layout: the extended trace is addressed as element (row, col) = src[row*rs + col*cs], so
+// the same kernel reads the column-major device LDE (rs = 1, cs = nrows; warp loads are
+// 256 B contiguous) or a row-major buffer (rs = ncols, cs = 1).
+#pragma once
+#include "poseidon2.cuh"
+#include "prof.cuh"
+
+namespace merkle {
+
+template <int W>
+__global__ void __launch_bounds__(128) leaf_hash_kernel(uint64_t *__restrict__ digests,
+                                                        const uint64_t *__restrict__ src, uint64_t rs,
+                                                        uint64_t cs, uint64_t ncols, uint64_t nrows)
+{
+    constexpr int RATE = W - 4;
+    const uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= nrows) return;
+    uint64_t st[W];
+#pragma unroll
+    for (int i = 0; i < W; i++) st[i] = 0;
+    const uint64_t *p = src + row * rs;
+    for (uint64_t done = 0; done < ncols; done += RATE) {
+        const uint64_t n = ncols - done;
+        if (done != 0) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) st[RATE + j] = st[j];
+        }
+        if (n >= (uint64_t)RATE) {
+#pragma unroll
+            for (int i = 0; i < RATE; i++) st[i] = __ldg(p + (done + i) * cs);
+        } else {
+#pragma unroll
+            for (int i = 0; i < RATE; i++) st[i] = (uint64_t)i < n ? __ldg(p + (done + i) * cs) : 0ull;
+        }
+        p2::permute<W>(st);
+    }
+    uint64_t *d = digests + row * 4;
+    // ncols == 0 leaves st zeroed: the zero digest
+    reinterpret_cast<ulonglong2 *>(d)[0] = make_ulonglong2(gl::canon(st[0]), gl::canon(st[1]));
+    reinterpret_cast<ulonglong2 *>(d)[1] = make_ulonglong2(gl::canon(st[2]), gl::canon(st[3]));
+}
+
+// One tree level: `pending` child digests at `level`, `pad` zero digests written after
+// them, `parents` parent digests written to `out` (= level + 4*(pending + pad)).
+template <int W>
+__global__ void __launch_bounds__(128) node_kernel(uint64_t *__restrict__ level, uint64_t pending, uint64_t pad,
+                                                   uint64_t parents, uint64_t *__restrict__ out)
+{
+    constexpr int ARITY = W / 4;
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= parents) return;
+    uint64_t st[W];
+#pragma unroll
+    for (int c = 0; c < ARITY; c++) {
+        const uint64_t child = i * ARITY + c;
+        if (child < pending) {
+            const ulonglong2 *q = reinterpret_cast<const ulonglong2 *>(level + child * 4);
+            ulonglong2 v0 = q[0], v1 = q[1];
+            st[4 * c + 0] = v0.x;
+            st[4 * c + 1] = v0.y;
+            st[4 * c + 2] = v1.x;
+            st[4 * c + 3] = v1.y;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) st[4 * c + j] = 0;
+        }
+    }
+    if (i == parents - 1) {
+        for (uint64_t z = 0; z < pad * 4; z++) level[pending * 4 + z] = 0;
+    }
+    p2::permute<W>(st);
+    uint64_t *d = out + i * 4;
+    reinterpret_cast<ulonglong2 *>(d)[0] = make_ulonglong2(gl::canon(st[0]), gl::canon(st[1]));
+    reinterpret_cast<ulonglong2 *>(d)[1] = make_ulonglong2(gl::canon(st[2]), gl::canon(st[3]));
+}
+
+// Whole Poseidon2 permutations of n independent states (permute / permuteTrunc checks).
+template <int W>
+__global__ void permute_kernel(uint64_t *__restrict__ out, const uint64_t *__restrict__ in, uint64_t n)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t st[W];
+#pragma unroll
+    for (int j = 0; j < W; j++) st[j] = in[i * W + j];
+    p2::permute<W>(st);
+#pragma unroll
+    for (int j = 0; j < W; j++) out[i * W + j] = gl::canon(st[j]);
+}
+
+inline uint64_t tree_num_elements(uint64_t nrows, uint64_t arity)
+{
+    uint64_t total = nrows, level = nrows;
+    while (level > 1) {
+        total += (arity - level % arity) % arity;
+        level = (level + arity - 1) / arity;
+        total += level;
+    }
+    return total * 4;
+}
+
+// Leaf digests and every level up to the root, on `stream`.
+template <int W>
+cudaError_t build_tree(uint64_t *d_tree, const uint64_t *d_src, uint64_t rs, uint64_t cs, uint64_t ncols,
+                       uint64_t nrows, cudaStream_t stream)
+{
+    constexpr uint64_t ARITY = W / 4;
+    if (nrows == 0) return cudaSuccess;
+    const unsigned tpb = 128;
+    {
+        prof::Scope ps(prof::LEAF_HASH, stream);
+        leaf_hash_kernel<W><<<(unsigned)((nrows + tpb - 1) / tpb), tpb, 0, stream>>>(d_tree, d_src, rs, cs, ncols,
+                                                                                       nrows);
+        prof::count();
+    }
+    prof::Scope ps(prof::TREE_LEVELS, stream);
+    uint64_t pending = nrows, base = 0;
+    while (pending > 1) {
+        const uint64_t pad = (ARITY - pending % ARITY) % ARITY;
+        const uint64_t parents = (pending + ARITY - 1) / ARITY;
+        uint64_t *lvl = d_tree + base;
+        node_kernel<W><<<(unsigned)((parents + tpb - 1) / tpb), tpb, 0, stream>>>(lvl, pending, pad, parents,
+                                                                                   lvl + (pending + pad) * 4);
+        prof::count();
+        base += (pending + pad) * 4;
+        pending = parents;
+    }
+    return cudaGetLastError();
+}
+
+inline cudaError_t build_tree_arity(uint64_t arity, uint64_t *d_tree, const uint64_t *d_src, uint64_t rs,
+                                    uint64_t cs, uint64_t ncols, uint64_t nrows, cudaStream_t stream)
+{
+    switch (arity) {
+    case 2: return build_tree<8>(d_tree, d_src, rs, cs, ncols, nrows, stream);
+    case 3: return build_tree<12>(d_tree, d_src, rs, cs, ncols, nrows, stream);
+    case 4: return build_tree<16>(d_tree, d_src, rs, cs, ncols, nrows, stream);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace merkle
