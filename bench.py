@@ -36,6 +36,9 @@ WORKLOADS = {
                nbits=22, nbits_ext=23, ncols=256, arity=4, sample_nbits=17),
     "c1": dict(desc="single AIR 2^16 x 32 base columns, blowup 2, Poseidon2 W16 arity-4 tree",
                nbits=16, nbits_ext=17, ncols=32, arity=4, sample_nbits=16),
+    # profiling case of the 256-column workload: LDE 2.1 GB (larger than L2), ~4.3 GB on the device
+    "c2s": dict(desc="single AIR 2^19 x 256 base columns, blowup 2, Poseidon2 W16 arity-4 tree",
+                nbits=19, nbits_ext=20, ncols=256, arity=4, sample_nbits=16),
 }
 METRIC = "LDE+Merkle commit GElem/s (NExt x nCols per second), bit-exact roots"
 UNIT = "GElem/s"
@@ -282,6 +285,10 @@ def run_ours(args, wl):
     kernel_ms = {k: round(v[0] / args.steps, 3) for k, v in cats.items()}
 
     # ---- end to end through the reference C ABI from pinned host memory ---------------
+    if args.no_e2e:
+        e2e = None
+        return finish(args, wl, pkg, dist, rank, world, value, ms, launches, kernel_ms, roofline, clocks, roots,
+                      None)
     host = torch.empty(N * ncols, dtype=torch.int64, pin_memory=True)
     host.copy_(trace)
     del trace, scratch, lde, tree
@@ -313,7 +320,15 @@ def run_ours(args, wl):
         raise RuntimeError("e2e roots differ from the resident-path root")
     e2e = world * elems * args.steps / e2e_s / 1e9
     bufs.close()
+    e2e_obj = {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": N * ncols * 8, "d2h_bytes_per_step": 32,
+               "api": "commit_witness + get_stream_proofs, 2 stream slots, pinned host trace"}
+    return finish(args, wl, pkg, dist, rank, world, value, ms, launches, kernel_ms, roofline, clocks, roots, e2e_obj)
 
+
+def finish(args, wl, pkg, dist, rank, world, value, ms, launches, kernel_ms, roofline, clocks, roots, e2e_obj):
+    nbits, nbe, ncols, arity = wl["nbits"], wl["nbits_ext"], wl["ncols"], wl["arity"]
+    N = 1 << nbits
+    w = 4 * arity
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
@@ -321,8 +336,7 @@ def run_ours(args, wl):
         "config": {"workload": wl["desc"], "nBits": nbits, "nBitsExt": nbe, "nCols": ncols, "arity": arity,
                    "hash": "Poseidon2 W%d" % w, "parallelism": "instance per GPU" if world > 1 else "single GPU",
                    "l2": "inputs (%.1f GB) larger than L2; no flush" % (N * ncols * 8 / 1e9)},
-        "e2e": {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": N * ncols * 8, "d2h_bytes_per_step": 32,
-                "api": "commit_witness + get_stream_proofs, 2 stream slots, pinned host trace"},
+        "e2e": e2e_obj,
         "gpu_launches": int(launches),
         "kernel_ms_per_step": kernel_ms,
         "roofline": roofline,
@@ -349,6 +363,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":

@@ -5,8 +5,8 @@
 // partially reduced (GL64_PARTIALLY_REDUCED, goldilocks/Makefile:134).  Canonical
 // form (x mod p) is produced only where values leave the library (gl_canon).
 //
-// The 64x64 product is formed from 32-bit IMAD/IMAD.HI carry chains and reduced
-// with 2^64 = 2^32 - 1 and 2^96 = -1 (mod p); no 64-bit multiply is used.
+// The 64x64 product is formed from four 32x32->64 multiply-adds (IMAD.WIDE), squares from
+// three, and reduced with 2^64 = 2^32 - 1 and 2^96 = -1 (mod p); no 64-bit multiply is used.
 // Reference semantics: goldilocks_base_field_scalar.hpp:16-41 (add/sub), :229-258 (mul).
 #pragma once
 #include <stdint.h>
@@ -47,22 +47,45 @@ __device__ __forceinline__ uint64_t reduce128(uint32_t r0, uint32_t r1, uint32_t
     return mk64(z0, z1);
 }
 
-// full 128-bit product of two 64-bit values, (r3:r2:r1:r0)
+// Full 128-bit product (r3:r2:r1:r0) from four 32x32->64 multiply-adds, each folding the
+// carry word of the previous one (no partial sum can exceed 2^64 - 1):
+//   t = a0*b1 + hi(a0*b0),  u = a1*b0 + lo(t),  w = a1*b1 + hi(t) + hi(u).
 __device__ __forceinline__ void mul128(uint64_t a, uint64_t b, uint32_t &r0, uint32_t &r1, uint32_t &r2,
                                        uint32_t &r3)
 {
-    uint32_t a0 = lo32(a), a1 = hi32(a), b0 = lo32(b), b1 = hi32(b);
-    asm("mul.lo.u32     %0, %4, %6;\n\t"
-        "mul.hi.u32     %1, %4, %6;\n\t"
-        "mad.lo.cc.u32  %1, %4, %7, %1;\n\t"
-        "madc.hi.u32    %2, %4, %7, 0;\n\t"
-        "mad.lo.cc.u32  %1, %5, %6, %1;\n\t"
-        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
-        "madc.hi.u32    %3, %5, %7, 0;\n\t"
-        "mad.lo.cc.u32  %2, %5, %7, %2;\n\t"
-        "addc.u32       %3, %3, 0;\n\t"
-        : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-        : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+    const uint32_t a0 = lo32(a), a1 = hi32(a), b0 = lo32(b), b1 = hi32(b);
+    uint64_t p00, t, u, w;
+    asm("mul.wide.u32 %0, %1, %2;" : "=l"(p00) : "r"(a0), "r"(b0));
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(t) : "r"(a0), "r"(b1), "l"(p00 >> 32));
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(u) : "r"(a1), "r"(b0), "l"((uint64_t)(uint32_t)t));
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(w) : "r"(a1), "r"(b1), "l"(t >> 32));
+    w += u >> 32;
+    r0 = lo32(p00);
+    r1 = lo32(u);
+    r2 = lo32(w);
+    r3 = hi32(w);
+}
+
+// a^2 = a0^2 + 2*a0*a1*2^32 + a1^2*2^64 with three wide products.
+__device__ __forceinline__ void sqr128(uint64_t a, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3)
+{
+    const uint32_t a0 = lo32(a), a1 = hi32(a);
+    uint64_t p00, c, w;
+    asm("mul.wide.u32 %0, %1, %2;" : "=l"(p00) : "r"(a0), "r"(a0));
+    asm("mul.wide.u32 %0, %1, %2;" : "=l"(c) : "r"(a0), "r"(a1));
+    // 2c = (cb : c2hi : c2lo)
+    const uint32_t c2lo = lo32(c) << 1, c2hi = __funnelshift_l(lo32(c), hi32(c), 1), cb = hi32(c) >> 31;
+    uint32_t s1, ad0, ad1;
+    asm("add.cc.u32  %0, %3, %4;\n\t"
+        "addc.cc.u32 %1, %5, 0;\n\t"
+        "addc.u32    %2, %6, 0;\n\t"
+        : "=r"(s1), "=r"(ad0), "=r"(ad1)
+        : "r"(hi32(p00)), "r"(c2lo), "r"(c2hi), "r"(cb));
+    asm("mad.wide.u32 %0, %1, %1, %2;" : "=l"(w) : "r"(a1), "l"(mk64(ad0, ad1)));
+    r0 = lo32(p00);
+    r1 = s1;
+    r2 = lo32(w);
+    r3 = hi32(w);
 }
 
 __device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b)
@@ -86,7 +109,12 @@ __device__ __forceinline__ uint64_t mul_add(uint64_t a, uint64_t b, uint64_t c)
     return reduce128(r0, r1, r2, r3);
 }
 
-__device__ __forceinline__ uint64_t sqr(uint64_t a) { return mul(a, a); }
+__device__ __forceinline__ uint64_t sqr(uint64_t a)
+{
+    uint32_t r0, r1, r2, r3;
+    sqr128(a, r0, r1, r2, r3);
+    return reduce128(r0, r1, r2, r3);
+}
 
 // a + b for loose a and loose b: a carry out of 2^64 is worth EPS; a second carry
 // (both operands near 2^64) is folded the same way and cannot repeat.

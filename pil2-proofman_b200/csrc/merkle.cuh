@@ -20,85 +20,91 @@
 
 namespace merkle {
 
+constexpr int TPB = 128;  // threads per CTA of the hashing kernels (one row / node / state each)
+
 template <int W>
-__global__ void __launch_bounds__(128) leaf_hash_kernel(uint64_t *__restrict__ digests,
+__global__ void __launch_bounds__(TPB) leaf_hash_kernel(uint64_t *__restrict__ digests,
                                                         const uint64_t *__restrict__ src, uint64_t rs,
                                                         uint64_t cs, uint64_t ncols, uint64_t nrows)
 {
     constexpr int RATE = W - 4;
-    const uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ uint64_t sm[W * TPB];
+    uint64_t *st = sm + threadIdx.x;
+    const uint64_t row = (uint64_t)blockIdx.x * TPB + threadIdx.x;
     if (row >= nrows) return;
-    uint64_t st[W];
 #pragma unroll
-    for (int i = 0; i < W; i++) st[i] = 0;
+    for (int i = 0; i < W; i++) st[i * TPB] = 0;
     const uint64_t *p = src + row * rs;
     for (uint64_t done = 0; done < ncols; done += RATE) {
         const uint64_t n = ncols - done;
         if (done != 0) {
 #pragma unroll
-            for (int j = 0; j < 4; j++) st[RATE + j] = st[j];
+            for (int j = 0; j < 4; j++) st[(RATE + j) * TPB] = st[j * TPB];
         }
         if (n >= (uint64_t)RATE) {
 #pragma unroll
-            for (int i = 0; i < RATE; i++) st[i] = __ldg(p + (done + i) * cs);
+            for (int i = 0; i < RATE; i++) st[i * TPB] = __ldg(p + (done + i) * cs);
         } else {
 #pragma unroll
-            for (int i = 0; i < RATE; i++) st[i] = (uint64_t)i < n ? __ldg(p + (done + i) * cs) : 0ull;
+            for (int i = 0; i < RATE; i++) st[i * TPB] = (uint64_t)i < n ? __ldg(p + (done + i) * cs) : 0ull;
         }
-        p2::permute<W>(st);
+        p2::permute_smem<W, TPB>(st);
     }
     uint64_t *d = digests + row * 4;
-    // ncols == 0 leaves st zeroed: the zero digest
-    reinterpret_cast<ulonglong2 *>(d)[0] = make_ulonglong2(gl::canon(st[0]), gl::canon(st[1]));
-    reinterpret_cast<ulonglong2 *>(d)[1] = make_ulonglong2(gl::canon(st[2]), gl::canon(st[3]));
+    // ncols == 0 leaves the state zeroed: the zero digest
+    reinterpret_cast<ulonglong2 *>(d)[0] = make_ulonglong2(gl::canon(st[0]), gl::canon(st[TPB]));
+    reinterpret_cast<ulonglong2 *>(d)[1] = make_ulonglong2(gl::canon(st[2 * TPB]), gl::canon(st[3 * TPB]));
 }
 
 // One tree level: `pending` child digests at `level`, `pad` zero digests written after
 // them, `parents` parent digests written to `out` (= level + 4*(pending + pad)).
 template <int W>
-__global__ void __launch_bounds__(128) node_kernel(uint64_t *__restrict__ level, uint64_t pending, uint64_t pad,
+__global__ void __launch_bounds__(TPB) node_kernel(uint64_t *__restrict__ level, uint64_t pending, uint64_t pad,
                                                    uint64_t parents, uint64_t *__restrict__ out)
 {
     constexpr int ARITY = W / 4;
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ uint64_t sm[W * TPB];
+    uint64_t *st = sm + threadIdx.x;
+    const uint64_t i = (uint64_t)blockIdx.x * TPB + threadIdx.x;
     if (i >= parents) return;
-    uint64_t st[W];
 #pragma unroll
     for (int c = 0; c < ARITY; c++) {
         const uint64_t child = i * ARITY + c;
         if (child < pending) {
             const ulonglong2 *q = reinterpret_cast<const ulonglong2 *>(level + child * 4);
-            ulonglong2 v0 = q[0], v1 = q[1];
-            st[4 * c + 0] = v0.x;
-            st[4 * c + 1] = v0.y;
-            st[4 * c + 2] = v1.x;
-            st[4 * c + 3] = v1.y;
+            const ulonglong2 v0 = q[0], v1 = q[1];
+            st[(4 * c + 0) * TPB] = v0.x;
+            st[(4 * c + 1) * TPB] = v0.y;
+            st[(4 * c + 2) * TPB] = v1.x;
+            st[(4 * c + 3) * TPB] = v1.y;
         } else {
 #pragma unroll
-            for (int j = 0; j < 4; j++) st[4 * c + j] = 0;
+            for (int j = 0; j < 4; j++) st[(4 * c + j) * TPB] = 0;
         }
     }
     if (i == parents - 1) {
         for (uint64_t z = 0; z < pad * 4; z++) level[pending * 4 + z] = 0;
     }
-    p2::permute<W>(st);
+    p2::permute_smem<W, TPB>(st);
     uint64_t *d = out + i * 4;
-    reinterpret_cast<ulonglong2 *>(d)[0] = make_ulonglong2(gl::canon(st[0]), gl::canon(st[1]));
-    reinterpret_cast<ulonglong2 *>(d)[1] = make_ulonglong2(gl::canon(st[2]), gl::canon(st[3]));
+    reinterpret_cast<ulonglong2 *>(d)[0] = make_ulonglong2(gl::canon(st[0]), gl::canon(st[TPB]));
+    reinterpret_cast<ulonglong2 *>(d)[1] = make_ulonglong2(gl::canon(st[2 * TPB]), gl::canon(st[3 * TPB]));
 }
 
 // Whole Poseidon2 permutations of n independent states (permute / permuteTrunc checks).
 template <int W>
-__global__ void permute_kernel(uint64_t *__restrict__ out, const uint64_t *__restrict__ in, uint64_t n)
+__global__ void __launch_bounds__(TPB) permute_kernel(uint64_t *__restrict__ out, const uint64_t *__restrict__ in,
+                                                      uint64_t n)
 {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ uint64_t sm[W * TPB];
+    uint64_t *st = sm + threadIdx.x;
+    const uint64_t i = (uint64_t)blockIdx.x * TPB + threadIdx.x;
     if (i >= n) return;
-    uint64_t st[W];
 #pragma unroll
-    for (int j = 0; j < W; j++) st[j] = in[i * W + j];
-    p2::permute<W>(st);
+    for (int j = 0; j < W; j++) st[j * TPB] = in[i * W + j];
+    p2::permute_smem<W, TPB>(st);
 #pragma unroll
-    for (int j = 0; j < W; j++) out[i * W + j] = gl::canon(st[j]);
+    for (int j = 0; j < W; j++) out[i * W + j] = gl::canon(st[j * TPB]);
 }
 
 inline uint64_t tree_num_elements(uint64_t nrows, uint64_t arity)
@@ -119,7 +125,7 @@ cudaError_t build_tree(uint64_t *d_tree, const uint64_t *d_src, uint64_t rs, uin
 {
     constexpr uint64_t ARITY = W / 4;
     if (nrows == 0) return cudaSuccess;
-    const unsigned tpb = 128;
+    const unsigned tpb = TPB;
     {
         prof::Scope ps(prof::LEAF_HASH, stream);
         leaf_hash_kernel<W><<<(unsigned)((nrows + tpb - 1) / tpb), tpb, 0, stream>>>(d_tree, d_src, rs, cs, ncols,

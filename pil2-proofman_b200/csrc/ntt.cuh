@@ -15,20 +15,18 @@
 //      and starts at stage b.  The last window writes canonical values.
 // A window covering butterfly stages [s0, s0+k) is a batch of independent 2^k-point
 // transforms over elements at stride 2^s0.  One CTA loads a 2^k x L tile (L consecutive
-// low-index lanes) into shared memory, runs the k radix-2 stages there with twiddles
-// w_{2^(t+1)}^j from a 2048-entry table, and applies the single inter-window twiddle
+// low-index lanes) into shared memory, applies the single inter-window twiddle
 // w_{2^(s0+k)}^(bitrev_k(mid)*lo) per element (before a DIT window, after a DIF window),
-// formed from a two-level table of w_{2^26} powers.
+// formed from a two-level table of w_{2^26} powers, and runs the k radix-2 stages as
+// register radix-16 phases (pass16_kernel below).
 #pragma once
 #include "gl64.cuh"
 #include "prof.cuh"
 
-#define NTT_KMAX 12   // widest window: inner twiddles w_{2^12}^j, j < 2048
+#define NTT_KMAX 12   // widest window (phase twiddles are powers of w_4096)
 #define NTT_TWLG 26   // inter-window twiddles: powers of w_{2^26}; transforms up to 2^26 points
 #define NTT_TILE_MAX 8192
 
-__device__ uint64_t g_ntt_inner_fwd[1 << (NTT_KMAX - 1)];
-__device__ uint64_t g_ntt_inner_inv[1 << (NTT_KMAX - 1)];
 __device__ uint64_t g_ntt_tw_lo_fwd[1 << 13];
 __device__ uint64_t g_ntt_tw_hi_fwd[1 << 13];
 __device__ uint64_t g_ntt_tw_lo_inv[1 << 13];
@@ -64,7 +62,144 @@ __device__ __forceinline__ uint64_t big_twiddle(uint64_t e, bool inv)
     return gl::mul(__ldg(lo + (e & 8191)), __ldg(hi + (e >> 13)));
 }
 
-__global__ void __launch_bounds__(512) pass_kernel(Pass a)
+// ---------------------------------------------------------------------------------
+// Window kernel with register radix-16 phases.
+//
+// The 2^k-point transform of a window is split into phases of r <= 4 stages.  In a
+// phase each thread takes the 2^r elements of one sub-transform (mid = hi|j<<pb|lo_m),
+// applies the phase twiddle w_{2^(pb+r)}^(bitrev_r(j)*lo_m) (before, DIT; after, DIF),
+// and runs the r radix-2 stages in registers with the compile-time roots w_2..w_16;
+// shared memory is touched once per phase instead of once per stage.  Shared memory is
+// padded by one word per 16 (index i -> i + i/16) so that a thread's 16 contiguous
+// elements of the first phase sit in different banks from its neighbours'.
+// ---------------------------------------------------------------------------------
+
+__device__ uint64_t g_ntt_w4096_fwd[4096];  // w_4096^i
+__device__ uint64_t g_ntt_w4096_inv[4096];  // w_4096^-i
+
+__device__ __forceinline__ uint32_t pad16(uint32_t i) { return i + (i >> 4); }
+
+// roots of unity of order <= 16 as compile-time constants: w_{2^(u+1)}^e (inverse if INV)
+template <bool INV>
+__device__ __forceinline__ uint64_t small_root(int u, int e)
+{
+    // w_16 = W[4] = 2^12 (goldilocks_base_field.cpp:16): F[e] = w_16^e, I[e] = w_16^-e mod p
+    constexpr uint64_t F[8] = {1ull, 4096ull, 16777216ull, 68719476736ull, 281474976710656ull,
+                               1152921504606846976ull, 1099511627520ull, 4503599626321920ull};
+    constexpr uint64_t I[8] = {1ull, 18442240469788262401ull, 18446742969902956801ull, 17293822564807737345ull,
+                               18446462594437873665ull, 18446744000695107585ull, 18446744069397807105ull,
+                               18446744069414580225ull};
+    const int idx = e << (3 - u);  // w_{2^(u+1)}^e = w_16^(e * 2^(3-u))
+    return INV ? I[idx] : F[idx];
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void radix_dit(uint64_t (&v)[16])
+{
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+        const int h = 1 << u;
+#pragma unroll
+        for (int j = 0; j < (1 << R); j++) {
+            if (j & h) continue;
+            const int e = j & (h - 1);
+            uint64_t x = v[j + h];
+            if (e) x = gl::mul(x, small_root<INV>(u, e));
+            const uint64_t y = v[j];
+            v[j] = gl::add(y, x);
+            v[j + h] = gl::sub(y, x);
+        }
+    }
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void radix_dif(uint64_t (&v)[16])
+{
+#pragma unroll
+    for (int u = R - 1; u >= 0; u--) {
+        const int h = 1 << u;
+#pragma unroll
+        for (int j = 0; j < (1 << R); j++) {
+            if (j & h) continue;
+            const int e = j & (h - 1);
+            const uint64_t y = v[j], x = v[j + h];
+            v[j] = gl::add(y, x);
+            uint64_t d = gl::sub(y, x);
+            if (e) d = gl::mul(d, small_root<INV>(u, e));
+            v[j + h] = d;
+        }
+    }
+}
+
+template <int R, bool DIF>
+__device__ __forceinline__ void radix_phase(uint64_t *sm, uint32_t k, uint32_t lgL, uint32_t pb)
+{
+    constexpr int NR = 1 << R;
+    const uint32_t T = 1u << (k + lgL);
+    const uint32_t Lm = (1u << lgL) - 1;
+    const uint64_t *wtab = DIF ? g_ntt_w4096_inv : g_ntt_w4096_fwd;
+    const uint32_t wsh = 12 - pb - R;  // w_{2^(pb+R)} = w_4096^(2^wsh)
+    for (uint32_t th = threadIdx.x; th < (T >> R); th += blockDim.x) {
+        const uint32_t l = th & Lm, g = th >> lgL;
+        const uint32_t lo_m = g & ((1u << pb) - 1), hi_m = g >> pb;
+        const uint32_t mbase = (hi_m << (pb + R)) | lo_m;
+        uint64_t v[16];
+#pragma unroll
+        for (int j = 0; j < NR; j++) v[j] = sm[pad16(((mbase | ((uint32_t)j << pb)) << lgL) | l)];
+        if (!DIF) {
+            if (pb && lo_m) {
+#pragma unroll
+                for (int j = 1; j < NR; j++) {
+                    const uint32_t br = __brev((uint32_t)j) >> (32 - R);
+                    v[j] = gl::mul(v[j], __ldg(wtab + (((br * lo_m) << wsh) & 4095)));
+                }
+            }
+            radix_dit<R, false>(v);
+        } else {
+            radix_dif<R, true>(v);
+            if (pb && lo_m) {
+#pragma unroll
+                for (int j = 1; j < NR; j++) {
+                    const uint32_t br = __brev((uint32_t)j) >> (32 - R);
+                    v[j] = gl::mul(v[j], __ldg(wtab + (((br * lo_m) << wsh) & 4095)));
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NR; j++) sm[pad16(((mbase | ((uint32_t)j << pb)) << lgL) | l)] = v[j];
+    }
+}
+
+template <bool DIF>
+__device__ __forceinline__ void run_phases(uint64_t *sm, uint32_t k, uint32_t lgL)
+{
+    // phases of 4 stages from the low mid bits (DIT) or from the high ones (DIF); the odd
+    // remainder is the last DIT phase / the first DIF phase
+    const uint32_t full = k >> 2, rem = k & 3;
+    if (!DIF) {
+        for (uint32_t ph = 0; ph < full; ph++) {
+            radix_phase<4, false>(sm, k, lgL, 4 * ph);
+            __syncthreads();
+        }
+        const uint32_t pb = 4 * full;
+        if (rem == 1) radix_phase<1, false>(sm, k, lgL, pb);
+        if (rem == 2) radix_phase<2, false>(sm, k, lgL, pb);
+        if (rem == 3) radix_phase<3, false>(sm, k, lgL, pb);
+        if (rem) __syncthreads();
+    } else {
+        const uint32_t pb = 4 * full;
+        if (rem == 1) radix_phase<1, true>(sm, k, lgL, pb);
+        if (rem == 2) radix_phase<2, true>(sm, k, lgL, pb);
+        if (rem == 3) radix_phase<3, true>(sm, k, lgL, pb);
+        if (rem) __syncthreads();
+        for (int ph = (int)full - 1; ph >= 0; ph--) {
+            radix_phase<4, true>(sm, k, lgL, 4 * ph);
+            __syncthreads();
+        }
+    }
+}
+
+__device__ __forceinline__ void pass16_body(const Pass &a)
 {
     extern __shared__ uint64_t sm[];
     const uint32_t k = a.k, lgL = a.lgL, s0 = a.s0;
@@ -88,37 +223,16 @@ __global__ void __launch_bounds__(512) pass_kernel(Pass a)
             const uint64_t E = (uint64_t)brev_bits(q >> lgL, k) * lo;
             if (E) v = gl::mul(v, big_twiddle(E << tw_shift, false));
         }
-        sm[q] = v;
+        sm[pad16(q)] = v;
     }
     __syncthreads();
-
-    const uint64_t *inner = inv ? g_ntt_inner_inv : g_ntt_inner_fwd;
-    const uint32_t nbf = T >> 1;
-    for (uint32_t step = 0; step < k; step++) {
-        const uint32_t t = inv ? (k - 1 - step) : step;
-        const uint32_t h = 1u << t;
-        for (uint32_t b = threadIdx.x; b < nbf; b += blockDim.x) {
-            const uint32_t l = b & Lm, mm = b >> lgL;
-            const uint32_t m = ((mm >> t) << (t + 1)) | (mm & (h - 1));
-            const uint32_t i1 = (m << lgL) | l, i2 = i1 + (h << lgL);
-            uint64_t u = sm[i1], v = sm[i2];
-            if (!inv) {
-                if (t) v = gl::mul(v, __ldg(inner + ((m & (h - 1)) << (NTT_KMAX - 1 - t))));
-                sm[i1] = gl::add(u, v);
-                sm[i2] = gl::sub(u, v);
-            } else {
-                sm[i1] = gl::add(u, v);
-                uint64_t d = gl::sub(u, v);
-                if (t) d = gl::mul(d, __ldg(inner + ((m & (h - 1)) << (NTT_KMAX - 1 - t))));
-                sm[i2] = d;
-            }
-        }
-        __syncthreads();
-    }
-
+    if (inv)
+        run_phases<true>(sm, k, lgL);
+    else
+        run_phases<false>(sm, k, lgL);
     for (uint32_t q = threadIdx.x; q < T; q += blockDim.x) {
         const uint64_t pos = base | ((uint64_t)(q >> lgL) << s0) | (q & Lm);
-        uint64_t v = sm[q];
+        uint64_t v = sm[pad16(q)];
         if (inv && s0 > 0) {
             const uint64_t lo = (lob << lgL) | (q & Lm);
             const uint64_t E = (uint64_t)brev_bits(q >> lgL, k) * lo;
@@ -134,6 +248,10 @@ __global__ void __launch_bounds__(512) pass_kernel(Pass a)
         D[pos] = v;
     }
 }
+
+// two CTAs of 512 threads per SM (<= 64 registers): one CTA's global loads overlap the other's
+// shared-memory phases
+__global__ void __launch_bounds__(512, 2) pass16_kernel(Pass a) { pass16_body(a); }
 
 // row-major (nrows x ncols) -> column-major with column stride dst_cs
 __global__ void __launch_bounds__(256) transpose_kernel(uint64_t *__restrict__ dst, const uint64_t *__restrict__ src,
@@ -190,11 +308,11 @@ inline cudaError_t launch_pass(const Pass &p, uint64_t ncols, cudaStream_t strea
 {
     const uint32_t T = 1u << (p.k + p.lgL);
     const uint64_t tiles = (1ull << p.lg) >> (p.k + p.lgL);
-    uint32_t threads = T / 2;
+    uint32_t threads = T / 16;  // one radix-16 group per thread and phase
     if (threads < 32) threads = 32;
     if (threads > 512) threads = 512;
     dim3 grid((unsigned)tiles, (unsigned)ncols);
-    pass_kernel<<<grid, threads, (size_t)T * 8, stream>>>(p);
+    pass16_kernel<<<grid, threads, (size_t)(T + T / 16) * 8, stream>>>(p);
     prof::count();
     return cudaGetLastError();
 }
@@ -277,17 +395,11 @@ inline cudaError_t lde(uint64_t *d_lde, const uint64_t *d_trace, bool trace_rowm
 // Twiddle and coset tables, computed on the host once per device.
 inline cudaError_t init_tables()
 {
-    static uint64_t inner_f[1 << (NTT_KMAX - 1)], inner_i[1 << (NTT_KMAX - 1)];
     static uint64_t lo_f[1 << 13], hi_f[1 << 13], lo_i[1 << 13], hi_i[1 << 13];
     static uint64_t sh_lo[1 << 12], sh_hi[1 << 14];
+    static uint64_t w4096_f[4096], w4096_i[4096];
     static bool ready = false;
     if (!ready) {
-        const uint64_t w12 = glh::root_of_unity(NTT_KMAX), w12i = glh::inv(w12);
-        inner_f[0] = inner_i[0] = 1;
-        for (int j = 1; j < (1 << (NTT_KMAX - 1)); j++) {
-            inner_f[j] = glh::mul(inner_f[j - 1], w12);
-            inner_i[j] = glh::mul(inner_i[j - 1], w12i);
-        }
         const uint64_t W = glh::root_of_unity(NTT_TWLG), Wi = glh::inv(W);
         const uint64_t W13 = glh::pow(W, 1 << 13), W13i = glh::pow(Wi, 1 << 13);
         lo_f[0] = lo_i[0] = hi_f[0] = hi_i[0] = 1;
@@ -301,17 +413,23 @@ inline cudaError_t init_tables()
         sh_lo[0] = sh_hi[0] = 1;
         for (int j = 1; j < (1 << 12); j++) sh_lo[j] = glh::mul(sh_lo[j - 1], 7);
         for (int j = 1; j < (1 << 14); j++) sh_hi[j] = glh::mul(sh_hi[j - 1], s4096);
+        const uint64_t w4096 = glh::root_of_unity(12), w4096i = glh::inv(w4096);
+        w4096_f[0] = w4096_i[0] = 1;
+        for (int j = 1; j < 4096; j++) {
+            w4096_f[j] = glh::mul(w4096_f[j - 1], w4096);
+            w4096_i[j] = glh::mul(w4096_i[j - 1], w4096i);
+        }
         ready = true;
     }
     cudaError_t e;
-    if ((e = cudaMemcpyToSymbol(g_ntt_inner_fwd, inner_f, sizeof(inner_f))) != cudaSuccess) return e;
-    if ((e = cudaMemcpyToSymbol(g_ntt_inner_inv, inner_i, sizeof(inner_i))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(g_ntt_tw_lo_fwd, lo_f, sizeof(lo_f))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(g_ntt_tw_hi_fwd, hi_f, sizeof(hi_f))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(g_ntt_tw_lo_inv, lo_i, sizeof(lo_i))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(g_ntt_tw_hi_inv, hi_i, sizeof(hi_i))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(g_ntt_sh_lo, sh_lo, sizeof(sh_lo))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(g_ntt_sh_hi, sh_hi, sizeof(sh_hi))) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(g_ntt_w4096_fwd, w4096_f, sizeof(w4096_f))) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(g_ntt_w4096_inv, w4096_i, sizeof(w4096_i))) != cudaSuccess) return e;
     return cudaSuccess;
 }
 

@@ -48,8 +48,9 @@ static int ensure_init_current()
     std::lock_guard<std::mutex> lk(g_init_mu);
     if (g_init_done[dev]) return B200_OK;
     CK(ntt::init_tables(), "ntt tables");
-    CK(cudaFuncSetAttribute(ntt::pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, NTT_TILE_MAX * 8),
-       "pass_kernel smem attribute");
+    CK(cudaFuncSetAttribute(ntt::pass16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (NTT_TILE_MAX + NTT_TILE_MAX / 16) * 8),
+       "pass16_kernel smem attribute");
     g_init_done[dev] = true;
     return B200_OK;
 }
@@ -197,7 +198,7 @@ extern "C" void b200_fill_random_host(uint64_t *buf, uint64_t n, uint64_t seed)
 
 extern "C" const char *b200_kernel_names(void)
 {
-    return "pass_kernel\ntranspose_kernel\nleaf_hash_kernel\nnode_kernel\npermute_kernel\nlde_rows_kernel\n"
+    return "pass16_kernel\ntranspose_kernel\nleaf_hash_kernel\nnode_kernel\npermute_kernel\nlde_rows_kernel\n"
            "fill_kernel\nimad_probe_kernel\n";
 }
 

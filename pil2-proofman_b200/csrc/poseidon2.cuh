@@ -1,4 +1,4 @@
-// Poseidon2 over Goldilocks, widths 8 / 12 / 16, register-resident state.
+// Poseidon2 over Goldilocks, widths 8 / 12 / 16.
 //
 // Round structure (poseidon2_goldilocks.cpp:9-41): initial external layer M_E, 4 full
 // rounds (add C, x^7 on every word, M_E), 22 partial rounds (x0 += c, x0 = x0^7,
@@ -56,56 +56,101 @@ __device__ __forceinline__ void m4(uint64_t a, uint64_t b, uint64_t c, uint64_t 
     y3 = r3;
 }
 
-template <int W>
-__device__ __forceinline__ void external_layer(uint64_t (&x)[W])
+// ---------------------------------------------------------------------------------
+// The permutation keeps each thread's W state words in shared memory at st[i*TPB] (TPB
+// threads interleaved: a warp touches 32 consecutive words, no bank conflicts) and runs
+// the rounds as short loops over groups of four words.  A fully unrolled register-state
+// version is ~27k instructions of straight-line code, far larger than the instruction
+// cache: its warps stalled on instruction fetch and it ran 1.3x slower.  (Holding a CTA's
+// warps together with a barrier per round was measured too and gave nothing.)
+// ---------------------------------------------------------------------------------
+
+template <int W, int TPB>
+__device__ __forceinline__ void external_layer_smem(uint64_t *st)
 {
-    gl::Acc y[W];
-#pragma unroll
-    for (int i = 0; i < W; i += 4) m4(x[i], x[i + 1], x[i + 2], x[i + 3], y[i], y[i + 1], y[i + 2], y[i + 3]);
-    gl::Acc s[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        s[j] = y[j];
-#pragma unroll
-        for (int i = 4 + j; i < W; i += 4) s[j] = gl::acc_add(s[j], y[i]);
+    gl::Acc s0 = {0, 0, 0}, s1 = {0, 0, 0}, s2 = {0, 0, 0}, s3 = {0, 0, 0};
+#pragma unroll 1
+    for (int q = 0; q < W; q += 4) {
+        gl::Acc y0, y1, y2, y3;
+        m4(st[(q + 0) * TPB], st[(q + 1) * TPB], st[(q + 2) * TPB], st[(q + 3) * TPB], y0, y1, y2, y3);
+        s0 = gl::acc_add(s0, y0);
+        s1 = gl::acc_add(s1, y1);
+        s2 = gl::acc_add(s2, y2);
+        s3 = gl::acc_add(s3, y3);
+        st[(q + 0) * TPB] = gl::acc_reduce(y0);
+        st[(q + 1) * TPB] = gl::acc_reduce(y1);
+        st[(q + 2) * TPB] = gl::acc_reduce(y2);
+        st[(q + 3) * TPB] = gl::acc_reduce(y3);
     }
-#pragma unroll
-    for (int i = 0; i < W; i++) x[i] = gl::acc_reduce(gl::acc_add(y[i], s[i & 3]));
+    const uint64_t t0 = gl::acc_reduce(s0), t1 = gl::acc_reduce(s1), t2 = gl::acc_reduce(s2),
+                   t3 = gl::acc_reduce(s3);
+#pragma unroll 1
+    for (int q = 0; q < W; q += 4) {
+        st[(q + 0) * TPB] = gl::acc_reduce(gl::acc_add6464(st[(q + 0) * TPB], t0));
+        st[(q + 1) * TPB] = gl::acc_reduce(gl::acc_add6464(st[(q + 1) * TPB], t1));
+        st[(q + 2) * TPB] = gl::acc_reduce(gl::acc_add6464(st[(q + 2) * TPB], t2));
+        st[(q + 3) * TPB] = gl::acc_reduce(gl::acc_add6464(st[(q + 3) * TPB], t3));
+    }
 }
 
-template <int W>
-__device__ __forceinline__ void full_round(uint64_t (&x)[W], const uint64_t *C)
-{
-#pragma unroll
-    for (int i = 0; i < W; i++) x[i] = gl::pow7(gl::add_c(x[i], C[i]));
-    external_layer<W>(x);
-}
-
-template <int W>
-__device__ __forceinline__ void partial_round(uint64_t (&x)[W], uint64_t c, const uint64_t *D)
-{
-    x[0] = gl::pow7(gl::add_c(x[0], c));
-    gl::Acc s = gl::acc_add6464(x[0], x[1]);
-#pragma unroll
-    for (int i = 2; i < W; i++) s = gl::acc_add64(s, x[i]);
-    uint64_t sum = gl::acc_reduce(s);
-#pragma unroll
-    for (int i = 0; i < W; i++) x[i] = gl::mul_add(x[i], D[i], sum);
-}
-
-// In-place permutation of a width-W state (poseidon2_goldilocks.cpp:9-41).
-template <int W>
-__device__ __forceinline__ void permute(uint64_t (&x)[W])
+template <int W, int TPB>
+__device__ __forceinline__ void permute_smem(uint64_t *st)
 {
     const uint64_t *C = Tab<W>::C();
     const uint64_t *D = Tab<W>::D();
-    external_layer<W>(x);
 #pragma unroll 1
-    for (int r = 0; r < 4; r++) full_round<W>(x, C + r * W);
+    for (int r = 0; r <= 8; r++) {
+        if (r > 0) {
+            const uint64_t *Cr = C + (r <= 4 ? (r - 1) * W : 4 * W + NPARTIAL + (r - 5) * W);
 #pragma unroll 1
-    for (int r = 0; r < NPARTIAL; r++) partial_round<W>(x, C[4 * W + r], D);
+            for (int q = 0; q < W; q += 4) {
+                uint64_t a = st[(q + 0) * TPB], b = st[(q + 1) * TPB], c = st[(q + 2) * TPB], d = st[(q + 3) * TPB];
+                a = gl::pow7(gl::add_c(a, Cr[q + 0]));
+                b = gl::pow7(gl::add_c(b, Cr[q + 1]));
+                c = gl::pow7(gl::add_c(c, Cr[q + 2]));
+                d = gl::pow7(gl::add_c(d, Cr[q + 3]));
+                st[(q + 0) * TPB] = a;
+                st[(q + 1) * TPB] = b;
+                st[(q + 2) * TPB] = c;
+                st[(q + 3) * TPB] = d;
+            }
+        }
+        external_layer_smem<W, TPB>(st);
+        if (r == 4) {
+            // partial rounds: x0 stays in a register; the other words stream through smem
+            uint64_t x0 = st[0];
 #pragma unroll 1
-    for (int r = 0; r < 4; r++) full_round<W>(x, C + 4 * W + NPARTIAL + r * W);
+            for (int pr = 0; pr < NPARTIAL; pr++) {
+                x0 = gl::pow7(gl::add_c(x0, C[4 * W + pr]));
+                gl::Acc s = gl::acc(x0);
+#pragma unroll 1
+                for (int q = 4; q < W + 4; q += 4) {
+                    const int i = q - 4;
+                    if (i) s = gl::acc_add64(s, st[(i + 0) * TPB]);
+                    s = gl::acc_add64(s, st[(i + 1) * TPB]);
+                    s = gl::acc_add64(s, st[(i + 2) * TPB]);
+                    s = gl::acc_add64(s, st[(i + 3) * TPB]);
+                }
+                const uint64_t sum = gl::acc_reduce(s);
+                x0 = gl::mul_add(x0, D[0], sum);
+                st[1 * TPB] = gl::mul_add(st[1 * TPB], D[1], sum);
+                st[2 * TPB] = gl::mul_add(st[2 * TPB], D[2], sum);
+                st[3 * TPB] = gl::mul_add(st[3 * TPB], D[3], sum);
+#pragma unroll 1
+                for (int q = 4; q < W; q += 4) {
+                    const uint64_t a = gl::mul_add(st[(q + 0) * TPB], D[q + 0], sum);
+                    const uint64_t b = gl::mul_add(st[(q + 1) * TPB], D[q + 1], sum);
+                    const uint64_t c = gl::mul_add(st[(q + 2) * TPB], D[q + 2], sum);
+                    const uint64_t d = gl::mul_add(st[(q + 3) * TPB], D[q + 3], sum);
+                    st[(q + 0) * TPB] = a;
+                    st[(q + 1) * TPB] = b;
+                    st[(q + 2) * TPB] = c;
+                    st[(q + 3) * TPB] = d;
+                }
+            }
+            st[0] = x0;
+        }
+    }
 }
 
 }  // namespace p2
