@@ -157,6 +157,21 @@ uint64_t b200_lde_scratch_words(uint64_t nBits, uint64_t nCols);
 int b200_lde_device(uint64_t *d_lde, const uint64_t *d_trace, int trace_rowmajor, uint64_t nBits,
                     uint64_t nBitsExt, uint64_t nCols, uint64_t *d_scratch, void *stream);
 
+/* The same LDE for callers that may not allocate device memory — a prover whose device
+ * memory all comes from its own pool or budget (torch's caching allocator, a preallocated
+ * arena), or a latency-critical loop that must not pay cudaMalloc's implicit device
+ * synchronisation.  No counterpart in the reference (its LDE allocates or borrows a
+ * buffer).  The scratch is a 64 MiB array inside this library's image, held by every GPU
+ * that loads the library until exit: N * nCols must be <= 2^23 (larger shapes return
+ * B200_EINVAL).  No cudaMalloc / cudaFree or other allocating call is made (with the
+ * optional kernel timers off, the default).  The first call on a device resolves the
+ * array's device address and uploads the twiddle tables; make that first call before any
+ * stream capture.  All calls share the one array, which keeps the last call's contents
+ * (nothing in it needs to start at zero): calls that overlap on the GPU — on different
+ * streams or from different threads — race and must be serialised by the caller. */
+int b200_lde_device_static_scratch(uint64_t *d_lde, const uint64_t *d_trace, int trace_rowmajor, uint64_t nBits,
+                                   uint64_t nBitsExt, uint64_t nCols, void *stream);
+
 /* Merkle tree (leaf sponge + levels) over element (row, col) = d_src[row*rs + col*cs]. */
 int b200_merkletree_device(uint64_t *d_tree, const uint64_t *d_src, uint64_t rs, uint64_t cs, uint64_t nCols,
                            uint64_t nRows, uint64_t arity, void *stream);

@@ -55,6 +55,7 @@ _SIGS = {
     "b200_tree_num_elements": (_u64, [_u64, _u64]),
     "b200_lde_scratch_words": (_u64, [_u64, _u64]),
     "b200_lde_device": (_i32, [_vp, _vp, _i32, _u64, _u64, _u64, _vp, _vp]),
+    "b200_lde_device_static_scratch": (_i32, [_vp, _vp, _i32, _u64, _u64, _u64, _vp]),
     "b200_merkletree_device": (_i32, [_vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp]),
     "b200_commit_device": (_i32, [_vp, _vp, _vp, _vp, _i32, _u64, _u64, _u64, _u64, _vp, _vp]),
     "b200_permute_device": (_i32, [_vp, _vp, _u64, _u64, _vp]),
@@ -145,6 +146,13 @@ def init(device=0):
 def lde_device(d_lde, d_trace, nbits, nbits_ext, ncols, d_scratch, trace_rowmajor=True, stream=None):
     _check(load().b200_lde_device(_ptr(d_lde), _ptr(d_trace), 1 if trace_rowmajor else 0, nbits, nbits_ext,
                                   ncols, _ptr(d_scratch), _stream(stream)))
+
+
+def lde_device_static_scratch(d_lde, d_trace, nbits, nbits_ext, ncols, trace_rowmajor=True, stream=None):
+    """LDE without any device allocation: the scratch is the library's built-in 64 MiB array
+    (N * nCols <= 2^23).  Calls share that array, so calls that overlap on the GPU race."""
+    _check(load().b200_lde_device_static_scratch(_ptr(d_lde), _ptr(d_trace), 1 if trace_rowmajor else 0, nbits,
+                                                 nbits_ext, ncols, _stream(stream)))
 
 
 def merkletree_device(d_tree, d_src, rs, cs, ncols, nrows, arity, stream=None):

@@ -103,6 +103,49 @@ extern "C" int b200_lde_device(uint64_t *d_lde, const uint64_t *d_trace, int tra
     return B200_OK;
 }
 
+// ---------------------------------------- LDE with the library's own scratch area ----
+// Some callers may not allocate device memory at all: a prover that hands the library only
+// buffers carved from its own pool (torch's caching allocator, a preallocated arena under a
+// fixed memory budget), or a latency-critical loop that cannot afford cudaMalloc's implicit
+// device synchronisation.  For them the LDE runs with a scratch area that is part of this
+// library's image: a file-scope device array, loaded with the module and held by every GPU
+// that loads the library until the process exits.
+#define B200_STATIC_SCRATCH_WORDS (1ull << 23)  // 64 MiB: N * nCols <= 2^23 words
+static __device__ __align__(256) uint64_t g_static_lde_scratch[B200_STATIC_SCRATCH_WORDS];
+static uint64_t *g_static_scratch_addr[64];  // device address of the array, per device
+static std::mutex g_static_scratch_mu;
+
+extern "C" int b200_lde_device_static_scratch(uint64_t *d_lde, const uint64_t *d_trace, int trace_rowmajor,
+                                              uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, void *stream)
+{
+    int rc = check_shape(nBits, nBitsExt, nCols, 4);
+    if (rc) return rc;
+    const uint64_t words = ntt::lde_scratch_words((uint32_t)nBits, nCols);
+    if (words > B200_STATIC_SCRATCH_WORDS)
+        return set_err(B200_EINVAL, "b200_lde_device_static_scratch: needs " + std::to_string(words) +
+                                        " scratch words, the built-in area holds " +
+                                        std::to_string(B200_STATIC_SCRATCH_WORDS) + " (N * nCols <= 2^23)");
+    if (nCols && (!d_lde || !d_trace)) return set_err(B200_EINVAL, "null buffer");
+    if ((rc = ensure_init_current())) return rc;
+    int dev = 0;
+    CK(cudaGetDevice(&dev), "cudaGetDevice");
+    uint64_t *scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_static_scratch_mu);
+        if (!g_static_scratch_addr[dev]) {
+            // the array's name is a host-side stand-in; the kernels need its device address
+            void *p = nullptr;
+            CK(cudaGetSymbolAddress(&p, g_static_lde_scratch), "cudaGetSymbolAddress(static LDE scratch)");
+            g_static_scratch_addr[dev] = (uint64_t *)p;
+        }
+        scratch = g_static_scratch_addr[dev];
+    }
+    CK(ntt::lde(d_lde, d_trace, trace_rowmajor != 0, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, scratch,
+                (cudaStream_t)stream),
+       "lde (static scratch)");
+    return B200_OK;
+}
+
 extern "C" int b200_merkletree_device(uint64_t *d_tree, const uint64_t *d_src, uint64_t rs, uint64_t cs,
                                       uint64_t nCols, uint64_t nRows, uint64_t arity, void *stream)
 {
