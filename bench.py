@@ -355,16 +355,129 @@ def finish(args, wl, pkg, dist, rank, world, value, ms, launches, kernel_ms, roo
     return 0
 
 
+def c3_shapes(seed=3, n=64):
+    """64 AIR instances: log2 rows uniform in 16..22, base columns uniform in [16, 512], blowup 2 for
+    48 of them and 4 for 16, arity 4 (the reference's production W16 pairing)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nbits = rng.integers(16, 23, size=n)
+    ncols = rng.integers(16, 513, size=n)
+    blow = np.array([1] * 48 + [2] * 16)
+    rng.shuffle(blow)
+    return [(int(a), int(a + b), int(c)) for a, b, c in zip(nbits, blow, ncols)]
+
+
+def instance_words(pkg, nb, nbe, nc, arity=4):
+    N, NExt = 1 << nb, 1 << nbe
+    return N * nc, N * nc, NExt * nc, pkg.tree_num_elements(NExt, arity)
+
+
+def run_batched(args):
+    """Batched mixed-size commit (64 instances) vs the plain one-instance-at-a-time path, same data,
+    same device, waves bounded by a device-memory budget; roots compared bit for bit."""
+    import torch
+
+    pkg = load_package()
+    pkg.init(0)
+    lib = pkg.load()
+    dev = torch.device("cuda", 0)
+    shapes = c3_shapes()
+    budget = int(args.budget_gb * 2**30) // 8  # words
+    waves, cur, used = [], [], 0
+    for i, (nb, nbe, nc) in enumerate(shapes):
+        w = sum(instance_words(pkg, nb, nbe, nc))
+        if cur and used + w > budget:
+            waves.append(cur)
+            cur, used = [], 0
+        cur.append(i)
+        used += w
+    waves.append(cur)
+    stream = torch.cuda.Stream()
+    total_elems = sum((1 << nbe) * nc for _, nbe, nc in shapes)
+    t_plain = t_batch = 0.0
+    launches_plain = launches_batch = 0
+    mismatches = 0
+    for wave in waves:
+        sizes = [instance_words(pkg, *shapes[i]) for i in wave]
+        arena = torch.empty(sum(sum(s) for s in sizes) + 64 * len(wave), dtype=torch.int64, device=dev)
+        base = arena.data_ptr()
+        descs = (pkg.BatchInstance * len(wave))()
+        off = 0
+        for j, i in enumerate(wave):
+            nb, nbe, nc = shapes[i]
+            ptrs = []
+            for words in sizes[j]:
+                ptrs.append(base + 8 * off)
+                off += words + 8  # keep 64-byte alignment slack
+            d = descs[j]
+            d.d_trace, d.d_scratch, d.d_lde, d.d_tree = ptrs
+            d.nBits, d.nBitsExt, d.nCols, d.arity = nb, nbe, nc, 4
+            pkg.fill_random_device(ptrs[0], (1 << nb) * nc, 5000 + i)
+        torch.cuda.synchronize()
+        # plain: one instance after another on one stream
+        roots_plain = np.zeros((len(wave), 4), dtype=np.uint64)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            for rep in range(2):  # warm-up, then timed
+                l0 = pkg.launch_count()
+                ev0.record(stream)
+                for j in range(len(wave)):
+                    d = descs[j]
+                    r = pkg.commit_device(d.d_lde, d.d_tree, d.d_trace, d.nBits, d.nBitsExt, d.nCols, 4, d.d_scratch,
+                                          stream=stream)
+                    roots_plain[j] = r
+                ev1.record(stream)
+                torch.cuda.synchronize()
+            t_plain += ev0.elapsed_time(ev1)
+            launches_plain += pkg.launch_count() - l0
+            # batched: grouped kernels + persistent leaves, captured once in a CUDA graph
+            plan = lib.b200_batch_plan_new(descs, len(wave))
+            if not plan:
+                raise RuntimeError(lib.b200_last_error().decode())
+            roots_batch = np.zeros((len(wave), 4), dtype=np.uint64)
+            for rep in range(2):
+                l0 = pkg.launch_count()
+                ev0.record(stream)
+                rc = lib.b200_batch_plan_run(plan, roots_batch.ctypes.data, stream.cuda_stream, 1)
+                ev1.record(stream)
+                torch.cuda.synchronize()
+                if rc:
+                    raise RuntimeError(lib.b200_last_error().decode())
+            t_batch += ev0.elapsed_time(ev1)
+            launches_batch += int(lib.b200_batch_plan_launches(plan))
+            lib.b200_batch_plan_free(plan)
+        mismatches += int((roots_plain != roots_batch).any(axis=1).sum())
+        del arena
+        torch.cuda.empty_cache()
+    line = {
+        "metric": METRIC + " - batched vs plain", "workload": "c3",
+        "value": round(total_elems / (t_batch * 1e-3) / 1e9, 4), "unit": UNIT,
+        "plain_value": round(total_elems / (t_plain * 1e-3) / 1e9, 4),
+        "batched_over_plain": round(t_plain / t_batch, 4),
+        "ms_batched": round(t_batch, 2), "ms_plain": round(t_plain, 2),
+        "instances": len(shapes), "waves": len(waves), "total_lde_elements": total_elems,
+        "launches_plain": launches_plain, "launches_batched": launches_batch,
+        "roots_bit_exact": mismatches == 0, "mismatched_roots": mismatches,
+        "config": {"workload": "64 AIR instances, log2 rows U{16..22}, cols U[16,512], blowup 2 (48) / 4 (16), "
+                               "Poseidon2 W16 arity 4, device budget %.0f GiB per wave" % args.budget_gb},
+        "n_gpus": 1, "higher_is_better": True, "dtype": "u64", "data": "synthetic (seeded uniform Goldilocks)",
+    }
+    print(json.dumps(line), flush=True)
+    return 0 if mismatches == 0 else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c3"], default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--budget-gb", type=float, default=120.0, help="device memory per wave (c3)")
     args = ap.parse_args()
+    if args.workload == "c3":
+        return run_batched(args)
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         return run_reference(args, wl)

@@ -198,6 +198,48 @@ void b200_fill_random_host(uint64_t *buf, uint64_t n, uint64_t seed);
 int b200_lde_rows_device(uint64_t *d_out, const uint64_t *d_lde, uint64_t NExt, uint64_t nCols,
                          const uint64_t *d_rows, uint64_t nrows_req, void *stream);
 
+/* ---- Batched commit of many instances (device buffers) ---------------------------------
+ * One plan covers a fixed set of instances (shapes and buffers).  A run performs, for all of
+ * them together: one grouped transpose launch, one grouped launch per NTT window index, one
+ * persistent leaf-sponge launch per arity (resident CTAs claim 128-row blocks of any instance
+ * from a device counter), one grouped launch per tree level, one root gather.  With use_graph
+ * the first run captures that sequence into a CUDA graph and later runs replay it (stream
+ * must then be a created stream).  Results are bit-identical to b200_commit_device per
+ * instance.  The batched counterpart of the reference's per-instance commit loop
+ * (starks_api.cu:1599-1795 run once per instance on a stream from the pool). */
+typedef struct B200BatchInstance {
+    const uint64_t *d_trace; /* row-major N x nCols */
+    uint64_t *d_scratch;     /* b200_lde_scratch_words(nBits, nCols) words */
+    uint64_t *d_lde;         /* out: column-major NExt x nCols */
+    uint64_t *d_tree;        /* out: b200_tree_num_elements(NExt, arity) words */
+    uint64_t nBits, nBitsExt, nCols, arity;
+} B200BatchInstance;
+
+void *b200_batch_plan_new(const B200BatchInstance *inst, uint64_t n);
+/* roots_host: n*4 words (may be NULL: then the call does not wait for the GPU) */
+int b200_batch_plan_run(void *plan, uint64_t *roots_host, void *stream, int use_graph);
+void b200_batch_plan_free(void *plan);
+uint64_t b200_batch_plan_launches(void *plan);
+int b200_commit_batch_device(const B200BatchInstance *inst, uint64_t n, uint64_t *roots_host, void *stream);
+
+/* ---- Commit server (continuous admission) ----------------------------------------------
+ * Requests (host row-major traces; pinned memory lets the copies overlap) are admitted in
+ * arrival order whenever one of `slots` streams is free and the request's device buffers fit
+ * in `budget_bytes`; admitted requests run concurrently on their own streams.  The LDE and
+ * tree of a finished request stay on the device (b200_server_buffers, for query reads) until
+ * b200_server_release.  The reference's stream pool + selectStream + get_stream_proofs loop
+ * (starks_api.cu:1138-1170, 2665-...) is the single-request counterpart. */
+void *b200_server_new(int device, uint64_t budget_bytes, uint32_t slots);
+/* returns a request id > 0, or B200_EBUSY if the request can never fit the budget */
+int64_t b200_server_submit(void *srv, const uint64_t *host_trace, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols,
+                           uint64_t arity, uint64_t *root_out);
+/* 1 done (latency_ms = completion - submission), 0 queued or running, < 0 error */
+int b200_server_status(void *srv, int64_t id, double *latency_ms);
+int b200_server_wait_all(void *srv, uint64_t timeout_ms);
+int b200_server_release(void *srv, int64_t id);
+int b200_server_buffers(void *srv, int64_t id, uint64_t **d_lde, uint64_t **d_tree);
+void b200_server_free(void *srv);
+
 /* Names of the kernels this library launches (for test evidence), newline separated. */
 const char *b200_kernel_names(void);
 

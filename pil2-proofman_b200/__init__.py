@@ -70,6 +70,18 @@ _SIGS = {
     "b200_timing_name": (ctypes.c_char_p, [_i32]),
     "b200_launch_count": (_u64, []),
     "b200_probe_imad": (_i32, [_u64, _u64, ctypes.POINTER(ctypes.c_double)]),
+    "b200_batch_plan_new": (_vp, [_vp, _u64]),
+    "b200_batch_plan_run": (_i32, [_vp, _vp, _vp, _i32]),
+    "b200_batch_plan_free": (None, [_vp]),
+    "b200_batch_plan_launches": (_u64, [_vp]),
+    "b200_commit_batch_device": (_i32, [_vp, _u64, _vp, _vp]),
+    "b200_server_new": (_vp, [_i32, _u64, ctypes.c_uint32]),
+    "b200_server_submit": (ctypes.c_int64, [_vp, _vp, _u64, _u64, _u64, _u64, _vp]),
+    "b200_server_status": (_i32, [_vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)]),
+    "b200_server_wait_all": (_i32, [_vp, _u64]),
+    "b200_server_release": (_i32, [_vp, ctypes.c_int64]),
+    "b200_server_buffers": (_i32, [_vp, ctypes.c_int64, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
+    "b200_server_free": (None, [_vp]),
 }
 
 _lib = None
@@ -211,6 +223,13 @@ class StepsParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in (
         "trace", "aux_trace", "publicInputs", "proofValues", "challenges", "airgroupValues", "airValues",
         "evals", "xDivXSub", "pConstPolsAddress", "pConstPolsExtendedTreeAddress", "pCustomCommitsFixed")]
+
+
+class BatchInstance(ctypes.Structure):
+    """B200BatchInstance: device buffers and shape of one instance of a batched commit."""
+    _fields_ = [("d_trace", ctypes.c_void_p), ("d_scratch", ctypes.c_void_p), ("d_lde", ctypes.c_void_p),
+                ("d_tree", ctypes.c_void_p), ("nBits", ctypes.c_uint64), ("nBitsExt", ctypes.c_uint64),
+                ("nCols", ctypes.c_uint64), ("arity", ctypes.c_uint64)]
 
 
 class StarkShape:

@@ -22,16 +22,13 @@ namespace merkle {
 
 constexpr int TPB = 128;  // threads per CTA of the hashing kernels (one row / node / state each)
 
+// Sponge of one row; st = this thread's state slot in a W x TPB shared array.
 template <int W>
-__global__ void __launch_bounds__(TPB) leaf_hash_kernel(uint64_t *__restrict__ digests,
-                                                        const uint64_t *__restrict__ src, uint64_t rs,
-                                                        uint64_t cs, uint64_t ncols, uint64_t nrows)
+__device__ __forceinline__ void leaf_row(uint64_t *st, uint64_t *__restrict__ digests,
+                                         const uint64_t *__restrict__ src, uint64_t rs, uint64_t cs, uint64_t ncols,
+                                         uint64_t row)
 {
     constexpr int RATE = W - 4;
-    __shared__ uint64_t sm[W * TPB];
-    uint64_t *st = sm + threadIdx.x;
-    const uint64_t row = (uint64_t)blockIdx.x * TPB + threadIdx.x;
-    if (row >= nrows) return;
 #pragma unroll
     for (int i = 0; i < W; i++) st[i * TPB] = 0;
     const uint64_t *p = src + row * rs;
@@ -56,17 +53,23 @@ __global__ void __launch_bounds__(TPB) leaf_hash_kernel(uint64_t *__restrict__ d
     reinterpret_cast<ulonglong2 *>(d)[1] = make_ulonglong2(gl::canon(st[2 * TPB]), gl::canon(st[3 * TPB]));
 }
 
-// One tree level: `pending` child digests at `level`, `pad` zero digests written after
-// them, `parents` parent digests written to `out` (= level + 4*(pending + pad)).
 template <int W>
-__global__ void __launch_bounds__(TPB) node_kernel(uint64_t *__restrict__ level, uint64_t pending, uint64_t pad,
-                                                   uint64_t parents, uint64_t *__restrict__ out)
+__global__ void __launch_bounds__(TPB) leaf_hash_kernel(uint64_t *__restrict__ digests,
+                                                        const uint64_t *__restrict__ src, uint64_t rs,
+                                                        uint64_t cs, uint64_t ncols, uint64_t nrows)
+{
+    __shared__ uint64_t sm[W * TPB];
+    const uint64_t row = (uint64_t)blockIdx.x * TPB + threadIdx.x;
+    if (row < nrows) leaf_row<W>(sm + threadIdx.x, digests, src, rs, cs, ncols, row);
+}
+
+// Parent i of one tree level: `pending` child digests at `level`, `pad` zero digests written
+// after them (by the last parent), parents written to `out` (= level + 4*(pending + pad)).
+template <int W>
+__device__ __forceinline__ void node_one(uint64_t *st, uint64_t *__restrict__ level, uint64_t pending, uint64_t pad,
+                                         uint64_t parents, uint64_t *__restrict__ out, uint64_t i)
 {
     constexpr int ARITY = W / 4;
-    __shared__ uint64_t sm[W * TPB];
-    uint64_t *st = sm + threadIdx.x;
-    const uint64_t i = (uint64_t)blockIdx.x * TPB + threadIdx.x;
-    if (i >= parents) return;
 #pragma unroll
     for (int c = 0; c < ARITY; c++) {
         const uint64_t child = i * ARITY + c;
@@ -89,6 +92,15 @@ __global__ void __launch_bounds__(TPB) node_kernel(uint64_t *__restrict__ level,
     uint64_t *d = out + i * 4;
     reinterpret_cast<ulonglong2 *>(d)[0] = make_ulonglong2(gl::canon(st[0]), gl::canon(st[TPB]));
     reinterpret_cast<ulonglong2 *>(d)[1] = make_ulonglong2(gl::canon(st[2 * TPB]), gl::canon(st[3 * TPB]));
+}
+
+template <int W>
+__global__ void __launch_bounds__(TPB) node_kernel(uint64_t *__restrict__ level, uint64_t pending, uint64_t pad,
+                                                   uint64_t parents, uint64_t *__restrict__ out)
+{
+    __shared__ uint64_t sm[W * TPB];
+    const uint64_t i = (uint64_t)blockIdx.x * TPB + threadIdx.x;
+    if (i < parents) node_one<W>(sm + threadIdx.x, level, pending, pad, parents, out, i);
 }
 
 // Whole Poseidon2 permutations of n independent states (permute / permuteTrunc checks).

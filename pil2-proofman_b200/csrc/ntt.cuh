@@ -199,19 +199,19 @@ __device__ __forceinline__ void run_phases(uint64_t *sm, uint32_t k, uint32_t lg
     }
 }
 
-__device__ __forceinline__ void pass16_body(const Pass &a)
+// One CTA: tile `tile` of column `col` of the window described by `a`.
+__device__ __forceinline__ void pass16_body(const Pass &a, uint64_t tile, uint64_t col)
 {
     extern __shared__ uint64_t sm[];
     const uint32_t k = a.k, lgL = a.lgL, s0 = a.s0;
     const uint32_t T = 1u << (k + lgL);
     const uint32_t Lm = (1u << lgL) - 1;
     const uint32_t nlob = s0 - lgL;
-    const uint64_t tile = blockIdx.x;
     const uint64_t hi = tile >> nlob;
     const uint64_t lob = tile & ((1ull << nlob) - 1);
     const uint64_t base = (hi << (s0 + k)) | (lob << lgL);
-    const uint64_t *S = a.src + (uint64_t)blockIdx.y * a.src_cs;
-    uint64_t *D = a.dst + (uint64_t)blockIdx.y * a.dst_cs;
+    const uint64_t *S = a.src + col * a.src_cs;
+    uint64_t *D = a.dst + col * a.dst_cs;
     const bool inv = a.dif != 0;
     const uint32_t tw_shift = NTT_TWLG - s0 - k;
 
@@ -251,14 +251,16 @@ __device__ __forceinline__ void pass16_body(const Pass &a)
 
 // two CTAs of 512 threads per SM (<= 64 registers): one CTA's global loads overlap the other's
 // shared-memory phases
-__global__ void __launch_bounds__(512, 2) pass16_kernel(Pass a) { pass16_body(a); }
+__global__ void __launch_bounds__(512, 2) pass16_kernel(Pass a) { pass16_body(a, blockIdx.x, blockIdx.y); }
 
-// row-major (nrows x ncols) -> column-major with column stride dst_cs
-__global__ void __launch_bounds__(256) transpose_kernel(uint64_t *__restrict__ dst, const uint64_t *__restrict__ src,
-                                                        uint64_t nrows, uint64_t ncols, uint64_t dst_cs)
+// row-major (nrows x ncols) -> column-major with column stride dst_cs; one 32x32 tile per
+// CTA of 32x8 threads
+__device__ __forceinline__ void transpose_tile(uint64_t *__restrict__ dst, const uint64_t *__restrict__ src,
+                                               uint64_t nrows, uint64_t ncols, uint64_t dst_cs, uint64_t rtile,
+                                               uint64_t ctile)
 {
     __shared__ uint64_t tile[32][33];
-    const uint64_t r0 = (uint64_t)blockIdx.x * 32, c0 = (uint64_t)blockIdx.y * 32;
+    const uint64_t r0 = rtile * 32, c0 = ctile * 32;
     const uint32_t tx = threadIdx.x, ty = threadIdx.y;
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -273,6 +275,12 @@ __global__ void __launch_bounds__(256) transpose_kernel(uint64_t *__restrict__ d
     }
 }
 
+__global__ void __launch_bounds__(256) transpose_kernel(uint64_t *__restrict__ dst, const uint64_t *__restrict__ src,
+                                                        uint64_t nrows, uint64_t ncols, uint64_t dst_cs)
+{
+    transpose_tile(dst, src, nrows, ncols, dst_cs, blockIdx.x, blockIdx.y);
+}
+
 // ------------------------------------------------------------------ host side ----
 
 struct Window {
@@ -280,7 +288,8 @@ struct Window {
 };
 
 // Windows covering stages [lo, hi).  The window that starts at `lo` keeps every lower lane
-// (lgL = lo) so its tile is one contiguous run; the others take 8 lanes (4 for 11-bit windows).
+// (lgL = lo) so its tile is one contiguous run; the others take as many lanes as fill an
+// 8192-element tile (at most all 2^s0 of them).
 inline int plan_windows(uint32_t lo, uint32_t hi, Window *w, int maxw)
 {
     int n = 0;
@@ -294,7 +303,7 @@ inline int plan_windows(uint32_t lo, uint32_t hi, Window *w, int maxw)
     uint32_t np = (rest + 10) / 11;
     for (uint32_t i = 0; i < np; i++) {
         uint32_t k = rest / (np - i) + ((rest % (np - i)) ? 1 : 0);
-        uint32_t lgL = k >= 11 ? 2 : 3;
+        uint32_t lgL = 13 - k;  // 2^k x L = 8192-element tiles: L-word contiguous runs
         if (lgL > s) lgL = s;
         if (n >= maxw) return -1;
         w[n++] = Window{s, k, lgL};

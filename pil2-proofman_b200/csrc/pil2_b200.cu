@@ -242,7 +242,8 @@ extern "C" void b200_fill_random_host(uint64_t *buf, uint64_t n, uint64_t seed)
 extern "C" const char *b200_kernel_names(void)
 {
     return "pass16_kernel\ntranspose_kernel\nleaf_hash_kernel\nnode_kernel\npermute_kernel\nlde_rows_kernel\n"
-           "fill_kernel\nimad_probe_kernel\n";
+           "fill_kernel\nimad_probe_kernel\ntranspose_grouped\npass_grouped\nleaf_persistent\n"
+           "node_grouped\ngather_roots\n";
 }
 
 // ------------------------------------------------------------ host-buffer API ----
@@ -701,3 +702,7 @@ extern "C" int b200_probe_imad(uint64_t blocks, uint64_t iters, double *gimad_pe
     return B200_OK;
 }
 
+
+// ---------------------------------------------------- batched commit and server ----
+#include "batch_api.cuh"
+#include "server.cuh"
