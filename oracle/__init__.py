@@ -82,9 +82,11 @@ class _Base:
 
 
 class Oracle(_Base):
-    """The C restatement in gl_oracle.c."""
+    """The C restatement in gl_oracle.c.  ``family`` selects the hash: 2 = Poseidon2 (default),
+    1 = Poseidon1 (the reference's set_hash_family values)."""
 
-    def __init__(self):
+    def __init__(self, family=2):
+        self.family = 1 if family == 1 else 2
         path = os.path.join(HERE, "libgl_oracle.so")
         if not os.path.exists(path):
             build(ref=False)
@@ -99,6 +101,9 @@ class Oracle(_Base):
             "orc_merkletree_reduce": [ctypes.c_uint, _vp, _vp, _u64, _u64],
             "orc_tree_num_elements": [_u64, _u64],
             "orc_root_of_unity": [ctypes.c_uint],
+            "orc_set_hash_family": [ctypes.c_int],
+            "orc_p1_permute": [ctypes.c_uint, _vp],
+            "orc_merkletree_w": [ctypes.c_uint, _vp, _vp, _u64, _u64, _u64],
             "orc_mul": [_u64, _u64],
             "orc_add": [_u64, _u64],
             "orc_sub": [_u64, _u64],
@@ -107,21 +112,38 @@ class Oracle(_Base):
             f.argtypes = args
         for name in ("orc_tree_num_elements", "orc_root_of_unity", "orc_mul", "orc_add", "orc_sub"):
             getattr(lib, name).restype = _u64
-        for name in ("orc_merkletree", "orc_merkletree_colmajor", "orc_merkletree_reduce"):
+        for name in ("orc_merkletree_w", "orc_merkletree", "orc_merkletree_colmajor", "orc_merkletree_reduce"):
             getattr(lib, name).restype = ctypes.c_int
         self.lib = lib
 
     def _lde(self, out, trace, n, next_, ncols):
         self.lib.orc_lde(_ptr(out), _ptr(trace), n, next_, ncols)
 
+    def _fam(self):
+        # the C library keeps the family in one global, like the reference's set_hash_family
+        self.lib.orc_set_hash_family(self.family)
+
     def _merkletree(self, tree, matrix, ncols, nrows, arity):
+        self._fam()
         return self.lib.orc_merkletree(_ptr(tree), _ptr(matrix), ncols, nrows, arity)
+
+    def merkletree_w(self, width, matrix, arity):
+        """Row-major matrix -> tree with sponge/node width `width` >= 4*arity (node input zero-padded)."""
+        self._fam()
+        matrix = np.ascontiguousarray(matrix, dtype=np.uint64)
+        nrows, ncols = matrix.shape
+        tree = np.zeros(tree_num_elements(nrows, arity), dtype=np.uint64)
+        if self.lib.orc_merkletree_w(width, _ptr(tree), _ptr(matrix) if matrix.size else None, ncols, nrows,
+                                     arity) != 0:
+            raise ValueError("unsupported width/arity")
+        return tree
 
     def merkletree_colmajor(self, cols, arity):
         """Column-major (ncols, nrows) -> tree."""
         cols = np.ascontiguousarray(cols, dtype=np.uint64)
         ncols, nrows = cols.shape
         tree = np.zeros(tree_num_elements(nrows, arity), dtype=np.uint64)
+        self._fam()
         if self.lib.orc_merkletree_colmajor(_ptr(tree), _ptr(cols), ncols, nrows, arity) != 0:
             raise ValueError("unsupported arity")
         return tree
@@ -134,16 +156,21 @@ class Oracle(_Base):
 
     def permute(self, state):
         st = np.ascontiguousarray(state, dtype=np.uint64).copy()
-        self.lib.orc_permute(len(st), _ptr(st))
+        if self.family == 1:
+            self.lib.orc_p1_permute(len(st), _ptr(st))
+        else:
+            self.lib.orc_permute(len(st), _ptr(st))
         return st
 
     def linear_hash(self, width, data):
+        self._fam()
         data = np.ascontiguousarray(data, dtype=np.uint64)
         out = np.zeros(4, dtype=np.uint64)
         self.lib.orc_linear_hash(width, _ptr(out), _ptr(data) if data.size else None, data.size)
         return out
 
     def merkletree_reduce(self, width, digests, arity):
+        self._fam()
         digests = np.ascontiguousarray(digests, dtype=np.uint64)
         root = np.zeros(4, dtype=np.uint64)
         if self.lib.orc_merkletree_reduce(width, _ptr(root), _ptr(digests), digests.size // 4, arity) != 0:
@@ -166,9 +193,11 @@ def _cpu_has_avx512():
 
 
 class RefCPU(_Base):
-    """The reference's CPU implementation, built unmodified into _ref/."""
+    """The reference's CPU implementation, built unmodified into _ref/.  ``family`` 1 selects
+    PoseidonGoldilocks<W> (Poseidon1), 2 Poseidon2Goldilocks<W>, as MerkleTreeGL::merkelize does."""
 
-    def __init__(self, threads=None):
+    def __init__(self, threads=None, family=2):
+        self.family = 1 if family == 1 else 2
         variant = "avx512" if _cpu_has_avx512() else "avx2"
         path = os.path.join(HERE, "_ref", "libpil2ref_%s.so" % variant)
         if not os.path.exists(path):
@@ -186,6 +215,10 @@ class RefCPU(_Base):
         lib.ref_set_threads.argtypes = [ctypes.c_int]
         lib.ref_max_threads.restype = ctypes.c_int
         lib.ref_canonicalize.argtypes = [_vp, _u64]
+        lib.ref_p1_permute.argtypes = [_u64, _vp, _vp]
+        lib.ref_p1_linear_hash.argtypes = [_u64, _vp, _vp, _u64]
+        lib.ref_p1_merkletree.argtypes = [_u64, _vp, _vp, _u64, _u64, _u64]
+        lib.ref_p1_merkletree.restype = ctypes.c_int
         self.lib = lib
         self.variant = variant
         if threads:
@@ -199,18 +232,31 @@ class RefCPU(_Base):
         self.lib.ref_lde(_ptr(out), _ptr(trace), n, next_, ncols, None, 1)
 
     def _merkletree(self, tree, matrix, ncols, nrows, arity):
+        if self.family == 1:
+            return self.lib.ref_p1_merkletree(0, _ptr(tree), _ptr(matrix), ncols, nrows, arity)
         return self.lib.ref_merkletree(_ptr(tree), _ptr(matrix), ncols, nrows, arity)
+
+    def merkletree_w(self, width, matrix, arity):
+        """Poseidon1 merkletree<width> with 4*arity <= width (row-major matrix)."""
+        matrix = np.ascontiguousarray(matrix, dtype=np.uint64)
+        nrows, ncols = matrix.shape
+        tree = np.zeros(tree_num_elements(nrows, arity), dtype=np.uint64)
+        if self.family != 1 or self.lib.ref_p1_merkletree(width, _ptr(tree), _ptr(matrix) if matrix.size else None,
+                                                          ncols, nrows, arity) != 0:
+            raise ValueError("unsupported width/arity")
+        return self.canon(tree)
 
     def permute(self, state):
         st = np.ascontiguousarray(state, dtype=np.uint64)
         out = np.zeros_like(st)
-        self.lib.ref_permute(len(st), _ptr(out), _ptr(st))
+        (self.lib.ref_p1_permute if self.family == 1 else self.lib.ref_permute)(len(st), _ptr(out), _ptr(st))
         return self.canon(out)
 
     def linear_hash(self, width, data):
         data = np.ascontiguousarray(data, dtype=np.uint64)
         out = np.zeros(4, dtype=np.uint64)
-        self.lib.ref_linear_hash(width, _ptr(out), _ptr(data) if data.size else None, data.size)
+        f = self.lib.ref_p1_linear_hash if self.family == 1 else self.lib.ref_linear_hash
+        f(width, _ptr(out), _ptr(data) if data.size else None, data.size)
         return self.canon(out)
 
     def merkletree_reduce(self, width, digests, arity):

@@ -13,11 +13,15 @@
  *   Poseidon2 permute    poseidon2_goldilocks.cpp:9-41 ; matmul_m4_/matmul_external_ poseidon2_goldilocks.hpp:201-240
  *   linear hash          poseidon2_goldilocks.cpp:42-77
  *   Merkle tree          poseidon2_goldilocks.cpp:129-175 ; getTreeNumElements goldilocks_tooling.hpp:9-21
+ *   Poseidon1 permute    poseidon_goldilocks.cpp:13-51 ; pow7/add_/prod_/dot_/mvp_ poseidon_goldilocks.hpp:137-224
+ *   Poseidon1 sponge     poseidon_goldilocks.cpp:53-89 ; tree :91-150 (node input zero-padded to W)
+ *   hash family switch   utils/hash_family.hpp:45-66 (set_hash_family: 1 = Poseidon1, 2 = Poseidon2)
  */
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
+#include "poseidon1_constants.h"
 #include "poseidon2_constants.h"
 
 #define GL_P 0xFFFFFFFF00000001ULL
@@ -246,6 +250,67 @@ void orc_permute(unsigned w, uint64_t *x)
     }
 }
 
+/* ---------------------------------------------------------- Poseidon1 ---- */
+
+static int g_family = 2; /* 1 = Poseidon1, 2 = Poseidon2 */
+
+void orc_set_hash_family(int family) { g_family = family == 1 ? 1 : 2; }
+int orc_hash_family(void) { return g_family; }
+
+/* out_i = sum_j mat[j][i] x_j (mat row-major w x w, applied transposed as mvp_ does) */
+static void p1_mvp(uint64_t *x, const uint64_t *mat, unsigned w)
+{
+    uint64_t y[16];
+    for (unsigned i = 0; i < w; i++) {
+        uint64_t acc = 0;
+        for (unsigned j = 0; j < w; j++) acc = gl_add(acc, gl_mul(mat[j * w + i], x[j]));
+        y[i] = acc;
+    }
+    memcpy(x, y, w * sizeof(uint64_t));
+}
+
+/* Poseidon1 permutation of a width-w state (w in 8, 12, 16), in place: add C_0; 3 x (x^7, add
+ * C_r, M); x^7, add C_4, P; 22 sparse partial rounds (x0^7 + c; x0' = <x, S_r[0..w)>;
+ * x_i += x0 * S_r[w-1+i] for i >= 1); 3 x (x^7, add C, M); x^7, M. */
+void orc_p1_permute(unsigned w, uint64_t *x)
+{
+    const uint64_t *C = w == 8 ? P1_C8 : w == 12 ? P1_C12 : P1_C16;
+    const uint64_t *M = w == 8 ? P1_M8 : w == 12 ? P1_M12 : P1_M16;
+    const uint64_t *P = w == 8 ? P1_P8 : w == 12 ? P1_P12 : P1_P16;
+    const uint64_t *S = w == 8 ? P1_S8 : w == 12 ? P1_S12 : P1_S16;
+    for (unsigned i = 0; i < w; i++) x[i] = gl_add(canon(x[i]), C[i]);
+    for (unsigned r = 0; r < 3; r++) {
+        for (unsigned i = 0; i < w; i++) x[i] = gl_add(sbox(x[i]), C[(r + 1) * w + i]);
+        p1_mvp(x, M, w);
+    }
+    for (unsigned i = 0; i < w; i++) x[i] = gl_add(sbox(x[i]), C[4 * w + i]);
+    p1_mvp(x, P, w);
+    for (unsigned r = 0; r < P1_NPARTIAL; r++) {
+        const uint64_t *Sr = S + (2 * w - 1) * r;
+        const uint64_t x0 = gl_add(sbox(x[0]), C[5 * w + r]);
+        x[0] = x0;
+        uint64_t s0 = 0;
+        for (unsigned i = 0; i < w; i++) s0 = gl_add(s0, gl_mul(x[i], Sr[i]));
+        for (unsigned i = 1; i < w; i++) x[i] = gl_add(x[i], gl_mul(x0, Sr[w - 1 + i]));
+        x[0] = s0;
+    }
+    for (unsigned r = 0; r < 3; r++) {
+        for (unsigned i = 0; i < w; i++) x[i] = gl_add(sbox(x[i]), C[5 * w + P1_NPARTIAL + r * w + i]);
+        p1_mvp(x, M, w);
+    }
+    for (unsigned i = 0; i < w; i++) x[i] = sbox(x[i]);
+    p1_mvp(x, M, w);
+}
+
+/* the permutation of the selected family */
+static void permute_fam(unsigned w, uint64_t *x)
+{
+    if (g_family == 1)
+        orc_p1_permute(w, x);
+    else
+        orc_permute(w, x);
+}
+
 /* Sponge over `size` words with stride `stride`: rate w-4, capacity 4.  The capacity starts
  * at zero; each later block carries the previous output's first 4 words into it; a short
  * last block is zero-filled; no length padding; size 0 gives the zero digest. */
@@ -262,7 +327,7 @@ static void linear_hash_strided(unsigned w, uint64_t out[4], const uint64_t *in,
         uint64_t n = size - done < rate ? size - done : rate;
         if (done > 0) memcpy(st + rate, st, 4 * sizeof(uint64_t));
         for (unsigned i = 0; i < rate; i++) st[i] = i < n ? canon(in[(done + i) * stride]) : 0;
-        orc_permute(w, st);
+        permute_fam(w, st);
         done += n;
     }
     memcpy(out, st, 4 * sizeof(uint64_t));
@@ -287,9 +352,8 @@ uint64_t orc_tree_num_elements(uint64_t nrows, uint64_t arity)
 /* Fold digests level by level up to the root, in the reference buffer layout:
  * [level 0 digests | zero pad | level 1 | pad | ... | root].  Parent i of a level hashes the
  * arity*4 = w contiguous words of its children with one permutation and keeps words 0..3. */
-static void build_levels(uint64_t *tree, uint64_t nleaves, uint64_t arity)
+static void build_levels_w(uint64_t *tree, uint64_t nleaves, uint64_t arity, unsigned w)
 {
-    unsigned w = (unsigned)(4 * arity);
     uint64_t pending = nleaves, base = 0;
     while (pending > 1) {
         uint64_t pad = (arity - pending % arity) % arity;
@@ -299,13 +363,19 @@ static void build_levels(uint64_t *tree, uint64_t nleaves, uint64_t arity)
 #pragma omp parallel for schedule(static)
         for (uint64_t i = 0; i < parents; i++) {
             uint64_t st[16];
-            memcpy(st, tree + base + i * w, w * sizeof(uint64_t));
-            orc_permute(w, st);
+            memset(st, 0, sizeof(st));
+            memcpy(st, tree + base + i * 4 * arity, 4 * arity * sizeof(uint64_t));
+            permute_fam(w, st);
             memcpy(dst + i * 4, st, 4 * sizeof(uint64_t));
         }
         base += (pending + pad) * 4;
         pending = parents;
     }
+}
+
+static void build_levels(uint64_t *tree, uint64_t nleaves, uint64_t arity)
+{
+    build_levels_w(tree, nleaves, arity, (unsigned)(4 * arity));
 }
 
 /* Merkle tree of an nrows x ncols matrix given by (row_stride, col_stride); W = 4 * arity */
@@ -331,6 +401,18 @@ int orc_merkletree(uint64_t *tree, const uint64_t *in, uint64_t ncols, uint64_t 
 int orc_merkletree_colmajor(uint64_t *tree, const uint64_t *in, uint64_t ncols, uint64_t nrows, uint64_t arity)
 {
     return merkletree_strided(tree, in, 1, nrows, ncols, nrows, arity);
+}
+
+/* row-major input, sponge and node width w with 4 * arity <= w (PoseidonGoldilocks<W>::merkletree
+ * pads each node's arity*4 child words with zeros up to W) */
+int orc_merkletree_w(unsigned w, uint64_t *tree, const uint64_t *in, uint64_t ncols, uint64_t nrows, uint64_t arity)
+{
+    if (arity < 2 || 4 * arity > w) return -1;
+    if (nrows == 0) return 0;
+#pragma omp parallel for schedule(static)
+    for (uint64_t r = 0; r < nrows; r++) linear_hash_strided(w, tree + r * 4, in + r * ncols, 1, ncols);
+    build_levels_w(tree, nrows, arity, w);
+    return 0;
 }
 
 int orc_merkletree_reduce(unsigned w, uint64_t root[4], const uint64_t *digests, uint64_t n, uint64_t arity)

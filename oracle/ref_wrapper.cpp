@@ -1,8 +1,8 @@
 // C entry points over the reference's own CPU implementation of the commit path.
 //
 // Test infrastructure: compiled by oracle/Makefile together with the unmodified
-// reference sources goldilocks_base_field.cpp, ntt_goldilocks.cpp and
-// poseidon2_goldilocks.cpp into oracle/_ref/libpil2ref_*.so.  Used by the tests
+// reference sources goldilocks_base_field.cpp, ntt_goldilocks.cpp, poseidon2_goldilocks.cpp and
+// poseidon_goldilocks.cpp into oracle/_ref/libpil2ref_*.so.  Used by the tests
 // as a second, independent checker of the CUDA path and by bench.py as the
 // timed reference CPU baseline.  Every function mirrors one reference call:
 //   ref_lde          -> NTT_Goldilocks::LDE                 (ntt_goldilocks.cpp:369-404)
@@ -10,6 +10,8 @@
 //   ref_merkletree   -> Poseidon2Goldilocks<W>::merkletree  (poseidon2_goldilocks.hpp:337-369),
 //                       W = 4*arity as MerkleTreeGL::merkelize picks it (merkleTreeGL.cpp:316-336)
 //   ref_commit       -> write_custom_commit_cpu             (api/starks_api.cpp:633-657)
+//   ref_p1_*         -> PoseidonGoldilocks<W> (Poseidon1)   (poseidon_goldilocks.hpp:30-76), the
+//                       hash family 1 branch of MerkleTreeGL::merkelize (merkleTreeGL.cpp:300-318)
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -18,6 +20,7 @@
 #include "goldilocks_tooling.hpp"
 #include "ntt_goldilocks.hpp"
 #include "poseidon2_goldilocks.hpp"
+#include "poseidon_goldilocks.hpp"
 
 using GE = Goldilocks::Element;
 
@@ -122,6 +125,43 @@ void ref_canonicalize(uint64_t *buf, uint64_t n)
 {
 #pragma omp parallel for
     for (uint64_t i = 0; i < n; i++) buf[i] = Goldilocks::toU64(((GE *)buf)[i]);
+}
+
+// ---- Poseidon1 (hash family 1) ----
+int ref_p1_permute(uint64_t width, uint64_t *out, const uint64_t *in)
+{
+    switch (width) {
+    case 8: PoseidonGoldilocks<8>::permute(*(GE(*)[8])out, *(const GE(*)[8])in, PoseidonMode::Scalar); return 0;
+    case 12: PoseidonGoldilocks<12>::permute(*(GE(*)[12])out, *(const GE(*)[12])in, PoseidonMode::Scalar); return 0;
+    case 16: PoseidonGoldilocks<16>::permute(*(GE(*)[16])out, *(const GE(*)[16])in, PoseidonMode::Scalar); return 0;
+    default: return -1;
+    }
+}
+
+int ref_p1_linear_hash(uint64_t width, uint64_t *out, const uint64_t *in, uint64_t size)
+{
+    std::vector<GE> tmp(size + 1);
+    if (size) std::memcpy(tmp.data(), in, size * 8);
+    switch (width) {
+    case 8: PoseidonGoldilocks<8>::linearHash((GE *)out, tmp.data(), size, PoseidonMode::Scalar); return 0;
+    case 12: PoseidonGoldilocks<12>::linearHash((GE *)out, tmp.data(), size, PoseidonMode::Scalar); return 0;
+    case 16: PoseidonGoldilocks<16>::linearHash((GE *)out, tmp.data(), size, PoseidonMode::Scalar); return 0;
+    default: return -1;
+    }
+}
+
+// width 0: W = 4*arity (MerkleTreeGL's choice); otherwise the given W with 4*arity <= W
+int ref_p1_merkletree(uint64_t width, uint64_t *tree, const uint64_t *input, uint64_t ncols, uint64_t nrows,
+                      uint64_t arity)
+{
+    const uint64_t w = width ? width : (uint64_t)width_for_arity(arity);
+    if (4 * arity > w) return -1;
+    switch (w) {
+    case 8: PoseidonGoldilocks<8>::merkletree((GE *)tree, (GE *)input, ncols, nrows, arity); return 0;
+    case 12: PoseidonGoldilocks<12>::merkletree((GE *)tree, (GE *)input, ncols, nrows, arity); return 0;
+    case 16: PoseidonGoldilocks<16>::merkletree((GE *)tree, (GE *)input, ncols, nrows, arity); return 0;
+    default: return -1;
+    }
 }
 
 }  // extern "C"

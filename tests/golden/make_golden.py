@@ -10,6 +10,10 @@ Two sources, both from the reference (run here, where it is mounted):
    * pil2-stark/src/goldilocks/tests/test_ntt_cpu.cpp:182-263 (LDE with an explicit
      coset shift 49 of a Fibonacci column, N=16 -> 32) and :264-350 / :351-412
      (LDE_block / extendePol: 8 Fibonacci-like columns, N=16 -> 32, column 0 values).
+   * pil2-stark/src/goldilocks/tests/test_poseidon_cpu.cpp:56-90,361-395 (Poseidon1: W12
+     permute of a Fibonacci / zero state, W12 linearHash of 128 Fibonacci words, W12 arity-2
+     merkletree roots of a 128 x 64 Fibonacci matrix and of 0-column matrices with 64 and 2^17
+     rows, W8 permute of 0..7 (plonky3 cross-check), W16 permute of 0..15).
 2. Outputs of the reference CPU implementation itself (NTT_Goldilocks::LDE and
    Poseidon2Goldilocks<W>::merkletree, compiled unmodified by oracle/Makefile) on
    seeded inputs: Merkle roots and an LDE digest per shape.
@@ -57,6 +61,16 @@ SEEDED = [
 ]
 
 
+# seeded Poseidon1 (hash family 1) commits, W = 4 * arity as MerkleTreeGL picks it
+SEEDED_P1 = [
+    (4, 5, 8, 4, 21),
+    (6, 7, 13, 3, 22),
+    (8, 9, 7, 2, 23),
+    (10, 11, 32, 4, 24),
+    (12, 14, 12, 4, 25),
+]
+
+
 def parse_helpers(text):
     out = {}
     for m in re.finditer(r"constexpr uint64_t (\w+)\[\d+\]\s*=\s*\{(.*?)\};", text, re.S):
@@ -70,6 +84,13 @@ def parse_lde_test(text, name):
     return [int(v, 16) for _, v in sorted(vals, key=lambda t: int(t[0]))]
 
 
+def parse_poseidon1(text):
+    out = {}
+    for m in re.finditer(r"constexpr uint64_t (\w+)\[\w+\]\s*=\s*\{(.*?)\};", text, re.S):
+        out[m.group(1)] = [int(v, 0) for v in re.findall(r"0[xX][0-9a-fA-F]+|\d+", m.group(2))]
+    return out
+
+
 def digest(a):
     return hashlib.sha256(np.ascontiguousarray(a, dtype="<u8").tobytes()).hexdigest()
 
@@ -79,9 +100,17 @@ def main():
         helpers = parse_helpers(f.read())
     with open(os.path.join(REF, "test_ntt_cpu.cpp")) as f:
         ntt_text = f.read()
+    with open(os.path.join(REF, "test_poseidon_cpu.cpp")) as f:
+        p1 = parse_poseidon1(f.read())
+    for name, n in (("PERMUTE_FIB_W12_GOLDEN", 12), ("PERMUTE_ZERO_W12_GOLDEN", 12),
+                    ("LINEAR_HASH_FIB128_W12_GOLDEN", 4), ("MERKLE_BINARY_FIB128x64_ROOT", 4),
+                    ("MERKLE_BINARY_EMPTY_64_ROOT", 4), ("MERKLE_BINARY_EMPTY_POT17_ROOT", 4),
+                    ("PERMUTE_W8_POSEIDON1_PLONKY3_GOLDEN", 8), ("PERMUTE_W16_POSEIDON1_GOLDEN", 16)):
+        assert len(p1[name]) == n, name
     kats = {
         "source": "reference test sources (test_helpers.hpp, test_ntt_cpu.cpp) and the reference CPU build",
         "poseidon2": helpers,
+        "poseidon1": p1,
         "lde_shift49_fib_16_32": parse_lde_test(ntt_text, "LDE"),
         "lde_block_16_32_col0": parse_lde_test(ntt_text, "LDE_block"),
         "extendePol_16_32_col0": parse_lde_test(ntt_text, "extendePol"),
@@ -103,6 +132,15 @@ def main():
         })
         print("seeded", nbits, nbits_ext, ncols, arity, [hex(int(v)) for v in root])
     kats["seeded_commits"] = seeded
+    ref1 = oracle.RefCPU(family=1)
+    seeded1 = []
+    for nbits, nbits_ext, ncols, arity, seed in SEEDED_P1:
+        trace = oracle.random_field((1 << nbits, ncols), seed)
+        root, lde, tree = ref1.commit(trace, nbits_ext, arity)
+        seeded1.append({"nBits": nbits, "nBitsExt": nbits_ext, "nCols": ncols, "arity": arity, "seed": seed,
+                        "root": [int(v) for v in root], "tree_sha256": digest(tree)})
+        print("seeded poseidon1", nbits, nbits_ext, ncols, arity, [hex(int(v)) for v in root])
+    kats["seeded_commits_poseidon1"] = seeded1
     kats["seeded_generator"] = "oracle.random_field: numpy PCG64(seed), uniform u64 rejected unless < p, row-major"
     with open(os.path.join(HERE, "reference_kats.json"), "w") as f:
         json.dump(kats, f, indent=1)

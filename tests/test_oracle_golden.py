@@ -132,3 +132,71 @@ def test_tree_num_elements(orc):
     for n in [1, 2, 3, 4, 5, 16, 17, 1 << 10, (1 << 10) + 3]:
         for ar in (2, 3, 4):
             assert oracle.tree_num_elements(n, ar) == orc.lib.orc_tree_num_elements(n, ar)
+
+
+# ---- Poseidon1 (hash family 1): the reference's test_poseidon_cpu.cpp goldens ----
+
+def _fib(n):
+    out = [0, 1]
+    while len(out) < n:
+        out.append((out[-1] + out[-2]) % oracle.P)
+    return np.array(out[:n], dtype=np.uint64)
+
+
+def _fib_rows(ncols, nrows):
+    """buildMerkleInput (test_poseidon_cpu.cpp:175-186): rows 0 and 1 are 1..ncols, then
+    row_j = row_{j-2} + row_{j-1}."""
+    m = np.zeros((nrows, ncols), dtype=object)
+    m[0] = m[1] = np.arange(1, ncols + 1)
+    for j in range(2, nrows):
+        m[j] = (m[j - 2] + m[j - 1]) % oracle.P
+    return m.astype(np.uint64)
+
+
+@pytest.fixture(scope="module")
+def orc1():
+    return oracle.Oracle(family=1)
+
+
+def test_p1_permute_goldens(orc1, kats):
+    g = kats["poseidon1"]
+    assert [int(v) for v in orc1.permute(_fib(12))] == g["PERMUTE_FIB_W12_GOLDEN"]
+    assert [int(v) for v in orc1.permute(np.zeros(12, dtype=np.uint64))] == g["PERMUTE_ZERO_W12_GOLDEN"]
+    assert [int(v) for v in orc1.permute(np.arange(8, dtype=np.uint64))] == g["PERMUTE_W8_POSEIDON1_PLONKY3_GOLDEN"]
+    assert [int(v) for v in orc1.permute(np.arange(16, dtype=np.uint64))] == g["PERMUTE_W16_POSEIDON1_GOLDEN"]
+
+
+def test_p1_linear_hash_golden(orc1, kats):
+    out = orc1.linear_hash(12, _fib(128))
+    assert [int(v) for v in out] == kats["poseidon1"]["LINEAR_HASH_FIB128_W12_GOLDEN"]
+    assert not orc1.linear_hash(12, np.zeros(0, dtype=np.uint64)).any()
+
+
+def test_p1_merkletree_goldens(orc1, kats):
+    g = kats["poseidon1"]
+    tree = orc1.merkletree_w(12, _fib_rows(128, 64), 2)
+    assert [int(v) for v in tree[-4:]] == g["MERKLE_BINARY_FIB128x64_ROOT"]
+    tree = orc1.merkletree_w(12, np.zeros((64, 0), dtype=np.uint64), 2)
+    assert [int(v) for v in tree[-4:]] == g["MERKLE_BINARY_EMPTY_64_ROOT"]
+    tree = orc1.merkletree_w(12, np.zeros((1 << 17, 0), dtype=np.uint64), 2)
+    assert [int(v) for v in tree[-4:]] == g["MERKLE_BINARY_EMPTY_POT17_ROOT"]
+
+
+def test_p1_seeded_roots(orc1, kats):
+    for case in kats["seeded_commits_poseidon1"]:
+        trace = oracle.random_field((1 << case["nBits"], case["nCols"]), case["seed"])
+        root, _, tree = orc1.commit(trace, case["nBitsExt"], case["arity"])
+        assert [int(v) for v in root] == case["root"], case
+        assert digest(tree) == case["tree_sha256"]
+
+
+def test_p1_oracle_matches_reference_build(orc1):
+    ref1 = oracle.RefCPU(family=1)
+    for w in (8, 12, 16):
+        st = oracle.random_field((w,), 100 + w)
+        assert (orc1.permute(st) == ref1.permute(st)).all()
+        data = oracle.random_field((3 * w + 1,), 200 + w)
+        assert (orc1.linear_hash(w, data) == ref1.linear_hash(w, data)).all()
+    m = oracle.random_field((100, 9), 7)
+    for w, arity in ((8, 2), (12, 2), (12, 3), (16, 2), (16, 3), (16, 4)):
+        assert (orc1.merkletree_w(w, m, arity) == ref1.merkletree_w(w, m, arity)).all(), (w, arity)
