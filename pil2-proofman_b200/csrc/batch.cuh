@@ -188,10 +188,11 @@ class Plan {
         for (size_t i = 0; i < inst.size(); i++) {
             ntt::Window w[8];
             const Inst &x = inst[i];
-            int nw = x.nBits ? ntt::plan_windows(0, x.nBits, w, 8) : 0;
+            const ntt::Tune tn = ntt::tuned(x.nBits, x.nBitsExt, x.nCols);
+            int nw = x.nBits ? ntt::plan_windows(0, x.nBits, w, 8, tn.kfirst, tn.krest) : 0;
             if (nw < 0) return false;
             dif[i].assign(w, w + nw);
-            nw = ntt::plan_windows(x.nBitsExt - x.nBits, x.nBitsExt, w, 8);
+            nw = ntt::plan_windows(x.nBitsExt - x.nBits, x.nBitsExt, w, 8, tn.kfirst, tn.krest);
             if (nw < 0) return false;
             dit[i].assign(w, w + nw);
             maxd = std::max(maxd, (int)dif[i].size());

@@ -23,6 +23,9 @@
 #include "gl64.cuh"
 #include "prof.cuh"
 
+#include <map>
+#include <mutex>
+
 #define NTT_KMAX 12   // widest window (phase twiddles are powers of w_4096)
 #define NTT_TWLG 26   // inter-window twiddles: powers of w_{2^26}; transforms up to 2^26 points
 #define NTT_TILE_MAX 8192
@@ -48,6 +51,9 @@ struct Pass {
     uint32_t rep;             // source position = dst position >> rep
     uint32_t dif;             // 1: inverse DIF window, 0: forward DIT window
     uint32_t post;            // POST_*
+    uint32_t gshift;          // source index = ((dst position >> rep) << gshift) + goff
+    uint64_t goff;
+    uint64_t scale;           // loads multiplied by this factor (0: no scaling)
 };
 
 __device__ __forceinline__ uint32_t brev_bits(uint32_t x, uint32_t bits)
@@ -217,7 +223,8 @@ __device__ __forceinline__ void pass16_body(const Pass &a, uint64_t tile, uint64
 
     for (uint32_t q = threadIdx.x; q < T; q += blockDim.x) {
         const uint64_t pos = base | ((uint64_t)(q >> lgL) << s0) | (q & Lm);
-        uint64_t v = S[pos >> a.rep];
+        uint64_t v = S[((pos >> a.rep) << a.gshift) + a.goff];
+        if (a.scale) v = gl::mul(v, a.scale);
         if (!inv && s0 > 0) {
             const uint64_t lo = (lob << lgL) | (q & Lm);
             const uint64_t E = (uint64_t)brev_bits(q >> lgL, k) * lo;
@@ -253,6 +260,212 @@ __device__ __forceinline__ void pass16_body(const Pass &a, uint64_t tile, uint64
 // shared-memory phases
 __global__ void __launch_bounds__(512, 2) pass16_kernel(Pass a) { pass16_body(a, blockIdx.x, blockIdx.y); }
 
+// ---------------------------------------------------------------------------------
+// Fixed-shape window kernels.  The same computation as pass16_body with the window's
+// width K and lane count 2^LGL known at compile time: every loop has a constant trip
+// count, every phase's shared-memory addresses are one per-thread base plus constant
+// offsets, and positions are 32-bit (transforms are at most 2^26 points).  The generic
+// kernel above serves the shapes that are not instantiated.
+// ---------------------------------------------------------------------------------
+
+template <int K, int LGL>
+struct Shape {
+    static constexpr int T = 1 << (K + LGL);
+    static constexpr int NT = (T / 16) < 32 ? 32 : (T / 16) > 512 ? 512 : (T / 16);
+};
+
+// padded shared-memory index of element (base + j * 2^M) for base with zero bits in
+// [M, M + R): for M >= 4 the padding of the sum splits, (b + j*2^M) + (b + j*2^M)/16 =
+// pad16(b) + j*(2^M + 2^(M-4)), so offsets are compile-time constants.
+template <int M>
+__device__ __forceinline__ uint32_t pad_off(uint32_t pbase, uint32_t base, int j)
+{
+    if (M >= 4) return pbase + (uint32_t)j * ((1u << M) + (1u << (M >= 4 ? M - 4 : 0)));
+    return pad16(base + ((uint32_t)j << M));
+}
+
+template <int R, bool DIF, int K, int LGL, int PB>
+__device__ __forceinline__ void radix_phase_fixed(uint64_t *sm)
+{
+    constexpr int NR = 1 << R;
+    constexpr int G = Shape<K, LGL>::T >> R;  // sub-transforms in the tile
+    constexpr int NT = Shape<K, LGL>::NT;
+    constexpr int IT = (G + NT - 1) / NT;
+    constexpr int M = PB + LGL;
+    const uint64_t *wtab = DIF ? g_ntt_w4096_inv : g_ntt_w4096_fwd;
+    constexpr int WSH = 12 - PB - R;  // w_{2^(PB+R)} = w_4096^(2^WSH)
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        const uint32_t th = threadIdx.x + (uint32_t)it * NT;
+        if ((G % NT) != 0 && th >= (uint32_t)G) break;
+        const uint32_t l = th & ((1u << LGL) - 1), g = th >> LGL;
+        const uint32_t lo_m = g & ((1u << PB) - 1), hi_m = g >> PB;
+        const uint32_t base = (((hi_m << (PB + R)) | lo_m) << LGL) | l;
+        const uint32_t pbase = pad16(base);
+        uint64_t v[16];
+#pragma unroll
+        for (int j = 0; j < NR; j++) v[j] = sm[pad_off<M>(pbase, base, j)];
+        if (!DIF) {
+            if (PB && lo_m) {
+#pragma unroll
+                for (int j = 1; j < NR; j++) {
+                    const uint32_t br = __brev((uint32_t)j) >> (32 - R);
+                    v[j] = gl::mul(v[j], __ldg(wtab + (((br * lo_m) << WSH) & 4095)));
+                }
+            }
+            radix_dit<R, false>(v);
+        } else {
+            radix_dif<R, true>(v);
+            if (PB && lo_m) {
+#pragma unroll
+                for (int j = 1; j < NR; j++) {
+                    const uint32_t br = __brev((uint32_t)j) >> (32 - R);
+                    v[j] = gl::mul(v[j], __ldg(wtab + (((br * lo_m) << WSH) & 4095)));
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NR; j++) sm[pad_off<M>(pbase, base, j)] = v[j];
+    }
+}
+
+// DIT: full phases from the low mid bits, then the remainder; DIF: the reverse order
+template <bool DIF, int K, int LGL, int PH>
+__device__ __forceinline__ void phases_fixed(uint64_t *sm)
+{
+    constexpr int FULL = K >> 2, REM = K & 3;
+    if constexpr (!DIF) {
+        if constexpr (PH < FULL) {
+            radix_phase_fixed<4, false, K, LGL, 4 * PH>(sm);
+            __syncthreads();
+            phases_fixed<false, K, LGL, PH + 1>(sm);
+        } else if constexpr (REM != 0) {
+            radix_phase_fixed<REM, false, K, LGL, 4 * FULL>(sm);
+            __syncthreads();
+        }
+    } else {
+        // PH counts down from FULL (the remainder phase) to 0
+        if constexpr (PH == FULL) {
+            if constexpr (REM != 0) {
+                radix_phase_fixed<REM, true, K, LGL, 4 * FULL>(sm);
+                __syncthreads();
+            }
+            if constexpr (FULL > 0) phases_fixed<true, K, LGL, FULL - 1>(sm);
+        } else {
+            radix_phase_fixed<4, true, K, LGL, 4 * PH>(sm);
+            __syncthreads();
+            if constexpr (PH > 0) phases_fixed<true, K, LGL, PH - 1>(sm);
+        }
+    }
+}
+
+template <int K, int LGL>
+__global__ void __launch_bounds__(Shape<K, LGL>::NT, 1024 / Shape<K, LGL>::NT) pass_fixed_kernel(Pass a)
+{
+    extern __shared__ uint64_t sm[];
+    constexpr int T = Shape<K, LGL>::T, NT = Shape<K, LGL>::NT;
+    constexpr int IT = (T + NT - 1) / NT;
+    constexpr uint32_t Lm = (1u << LGL) - 1;
+    const uint32_t tile = blockIdx.x;
+    const uint64_t col = blockIdx.y;
+    const uint32_t s0 = a.s0;
+    const uint32_t nlob = s0 - LGL;
+    const uint32_t hi = tile >> nlob, lob = tile & ((1u << nlob) - 1);
+    const uint32_t base = (hi << (s0 + K)) | (lob << LGL);
+    const uint64_t *S = a.src + col * a.src_cs;
+    uint64_t *D = a.dst + col * a.dst_cs;
+    const bool inv = a.dif != 0;
+    const uint32_t tw_shift = NTT_TWLG - s0 - K;
+    const uint32_t rep = a.rep, gshift = a.gshift, goff = (uint32_t)a.goff;
+
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        const uint32_t q = threadIdx.x + (uint32_t)it * NT;
+        if ((T % NT) != 0 && q >= (uint32_t)T) break;
+        const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
+        uint64_t v = S[((pos >> rep) << gshift) + goff];
+        if (a.scale) v = gl::mul(v, a.scale);
+        if (!inv && s0 > 0) {
+            const uint32_t lo = (lob << LGL) | (q & Lm);
+            const uint32_t E = (__brev(q >> LGL) >> (32 - K)) * lo;
+            if (E) v = gl::mul(v, big_twiddle((uint64_t)(E << tw_shift), false));
+        }
+        sm[pad16(q)] = v;
+    }
+    __syncthreads();
+    if (inv)
+        phases_fixed<true, K, LGL, (K >> 2)>(sm);
+    else
+        phases_fixed<false, K, LGL, 0>(sm);
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        const uint32_t q = threadIdx.x + (uint32_t)it * NT;
+        if ((T % NT) != 0 && q >= (uint32_t)T) break;
+        const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
+        uint64_t v = sm[pad16(q)];
+        if (inv && s0 > 0) {
+            const uint32_t lo = (lob << LGL) | (q & Lm);
+            const uint32_t E = (__brev(q >> LGL) >> (32 - K)) * lo;
+            if (E) v = gl::mul(v, big_twiddle((uint64_t)(E << tw_shift), true));
+        }
+        if (a.post == POST_COSET) {
+            const uint32_t br = brev_bits(pos, a.lg);
+            const uint64_t f = gl::mul(__ldg(g_ntt_sh_lo + (br & 4095)), __ldg(g_ntt_sh_hi + (br >> 12)));
+            v = gl::mul(v, gl::mul(f, a.ninv));
+        } else if (a.post == POST_CANON) {
+            v = gl::canon(v);
+        }
+        D[pos] = v;
+    }
+}
+
+typedef void (*PassKernel)(Pass);
+
+// Instantiated shapes: full 8192-element tiles (K + LGL = 13: every window of a large
+// transform but the inverse's first) and single-lane windows (LGL = 0: the inverse's first).
+template <int K>
+inline PassKernel fixed_kernel_k(uint32_t lgL)
+{
+    if (lgL == 13 - K) return pass_fixed_kernel<K, 13 - K>;
+    if (lgL == 0) return pass_fixed_kernel<K, 0>;
+    return nullptr;
+}
+
+inline PassKernel fixed_kernel(uint32_t k, uint32_t lgL)
+{
+    switch (k) {
+    case 1: return fixed_kernel_k<1>(lgL);
+    case 2: return fixed_kernel_k<2>(lgL);
+    case 3: return fixed_kernel_k<3>(lgL);
+    case 4: return fixed_kernel_k<4>(lgL);
+    case 5: return fixed_kernel_k<5>(lgL);
+    case 6: return fixed_kernel_k<6>(lgL);
+    case 7: return fixed_kernel_k<7>(lgL);
+    case 8: return fixed_kernel_k<8>(lgL);
+    case 9: return fixed_kernel_k<9>(lgL);
+    case 10: return fixed_kernel_k<10>(lgL);
+    case 11: return fixed_kernel_k<11>(lgL);
+    case 12: return fixed_kernel_k<12>(lgL);
+    default: return nullptr;
+    }
+}
+
+// dynamic shared memory limit of every instantiated shape (tiles above 48 KB need the opt-in)
+inline cudaError_t set_fixed_attrs()
+{
+    for (uint32_t k = 1; k <= NTT_KMAX; k++) {
+        const uint32_t shapes[2] = {13 - k, 0};
+        for (uint32_t lgL : shapes) {
+            PassKernel kf = fixed_kernel(k, lgL);
+            if (!kf) continue;
+            const uint32_t T = 1u << (k + lgL);
+            cudaError_t e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (T + T / 16) * 8);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
+}
+
 // row-major (nrows x ncols) -> column-major with column stride dst_cs; one 32x32 tile per
 // CTA of 32x8 threads
 __device__ __forceinline__ void transpose_tile(uint64_t *__restrict__ dst, const uint64_t *__restrict__ src,
@@ -287,20 +500,62 @@ struct Window {
     uint32_t s0, k, lgL;
 };
 
+// Plan parameters per shape, filled by the autotuner (b200_autotune_lde): the largest first
+// window and the largest later windows.  Shapes never tuned use the defaults.
+struct Tune {
+    uint32_t kfirst = NTT_KMAX, krest = 11;
+};
+
+inline std::mutex &tune_mu()
+{
+    static std::mutex m;
+    return m;
+}
+
+inline std::map<uint64_t, Tune> &tune_table()
+{
+    static std::map<uint64_t, Tune> t;
+    return t;
+}
+
+// column counts are bucketed: the plan depends on the transform length, the grid on the width
+inline uint64_t tune_key(uint32_t nBits, uint32_t nBitsExt, uint64_t ncols)
+{
+    const uint64_t bucket = ncols <= 32 ? 0 : ncols <= 128 ? 1 : ncols <= 512 ? 2 : 3;
+    return (uint64_t)nBits | ((uint64_t)nBitsExt << 8) | (bucket << 16);
+}
+
+inline Tune tuned(uint32_t nBits, uint32_t nBitsExt, uint64_t ncols)
+{
+    std::lock_guard<std::mutex> lk(tune_mu());
+    auto it = tune_table().find(tune_key(nBits, nBitsExt, ncols));
+    return it == tune_table().end() ? Tune{} : it->second;
+}
+
+inline void set_tuned(uint32_t nBits, uint32_t nBitsExt, uint64_t ncols, Tune t)
+{
+    std::lock_guard<std::mutex> lk(tune_mu());
+    tune_table()[tune_key(nBits, nBitsExt, ncols)] = t;
+}
+
 // Windows covering stages [lo, hi).  The window that starts at `lo` keeps every lower lane
 // (lgL = lo) so its tile is one contiguous run; the others take as many lanes as fill an
-// 8192-element tile (at most all 2^s0 of them).
-inline int plan_windows(uint32_t lo, uint32_t hi, Window *w, int maxw)
+// 8192-element tile (at most all 2^s0 of them).  kfirst / krest cap the first window and the
+// others (the autotuned plan parameters).
+inline int plan_windows(uint32_t lo, uint32_t hi, Window *w, int maxw, uint32_t kfirst = NTT_KMAX,
+                        uint32_t krest = 11)
 {
     int n = 0;
     uint32_t total = hi - lo;
     uint32_t k0 = total;
+    if (k0 > kfirst) k0 = kfirst;
     if (k0 > NTT_KMAX) k0 = NTT_KMAX;
     if (k0 + lo > 13) k0 = (lo >= 13) ? 0 : 13 - lo;
     if (k0 == 0 && total > 0) return -1;  // stage offset too large for one tile
+    if (krest < 1 || krest > NTT_KMAX) krest = 11;
     w[n++] = Window{lo, k0, lo};
     uint32_t rest = total - k0, s = lo + k0;
-    uint32_t np = (rest + 10) / 11;
+    uint32_t np = (rest + krest - 1) / krest;
     for (uint32_t i = 0; i < np; i++) {
         uint32_t k = rest / (np - i) + ((rest % (np - i)) ? 1 : 0);
         uint32_t lgL = 13 - k;  // 2^k x L = 8192-element tiles: L-word contiguous runs
@@ -321,7 +576,12 @@ inline cudaError_t launch_pass(const Pass &p, uint64_t ncols, cudaStream_t strea
     if (threads < 32) threads = 32;
     if (threads > 512) threads = 512;
     dim3 grid((unsigned)tiles, (unsigned)ncols);
-    pass16_kernel<<<grid, threads, (size_t)(T + T / 16) * 8, stream>>>(p);
+    const size_t smem = (size_t)(T + T / 16) * 8;
+    if (PassKernel kf = fixed_kernel(p.k, p.lgL)) {
+        kf<<<grid, threads, smem, stream>>>(p);
+    } else {
+        pass16_kernel<<<grid, threads, smem, stream>>>(p);
+    }
     prof::count();
     return cudaGetLastError();
 }
@@ -353,7 +613,8 @@ inline cudaError_t lde(uint64_t *d_lde, const uint64_t *d_trace, bool trace_rowm
 
     // inverse DIF over [0, nBits), windows applied from the top stage down
     Window w[8];
-    int nw = nBits ? plan_windows(0, nBits, w, 8) : 0;
+    const Tune tn = tuned(nBits, nBitsExt, ncols);
+    int nw = nBits ? plan_windows(0, nBits, w, 8, tn.kfirst, tn.krest) : 0;
     if (nw < 0) return cudaErrorInvalidValue;
     const uint64_t ninv = glh::inv(N % GL_P);
     {
@@ -379,7 +640,7 @@ inline cudaError_t lde(uint64_t *d_lde, const uint64_t *d_trace, bool trace_rowm
     }
 
     // forward DIT over [b, nBitsExt) with replication by 2^b on the first window
-    nw = plan_windows(b, nBitsExt, w, 8);
+    nw = plan_windows(b, nBitsExt, w, 8, tn.kfirst, tn.krest);
     if (nw < 0) return cudaErrorInvalidValue;
     prof::Scope ps(prof::NTT_FWD, stream);
     for (int i = 0; i < nw; i++) {
@@ -397,6 +658,93 @@ inline cudaError_t lde(uint64_t *d_lde, const uint64_t *d_trace, bool trace_rowm
         p.dif = 0;
         p.post = (i == nw - 1) ? POST_CANON : POST_NONE;
         if ((err = launch_pass(p, ncols, stream)) != cudaSuccess) return err;
+    }
+    return cudaSuccess;
+}
+
+// Q-stage extension (Starks::computeQ, starks.hpp:186-239; GPU computeQColMajor,
+// ntt_goldilocks.cu:1515-1544): q holds qDim columns of NExt evaluations; their inverse NTT
+// over NExt gives coefficients c, which are cut into qDeg chunks of N, chunk p scaled by
+// S[p] = (7^-1)^(N*p), zero-padded to NExt and forward-transformed; cmQ column p*qDim + k is
+// chunk p of limb k.  Here the inverse DIF leaves c in bit-reversed order (position P holds
+// NExt*c[bitrev(P)]); the coefficient p*N + i sits at P = (bitrev_n(i) << b) | bitrev_b(p), so the
+// first forward window of chunk p gathers positions (q << b) | bitrev_b(p) and scales them by
+// S[p]/NExt — the zero padding and the first b forward stages fold away as in lde().
+// d_cmq: column-major NExt x (qDeg*qDim); d_q: column-major NExt x qDim (or row-major);
+// d_scratch: NExt * qDim words.  Requires qDeg <= NExt/N.
+inline cudaError_t lde_q(uint64_t *d_cmq, const uint64_t *d_q, bool q_rowmajor, uint32_t nBits, uint32_t nBitsExt,
+                         uint32_t qDeg, uint32_t qDim, uint64_t *d_scratch, cudaStream_t stream)
+{
+    if (qDim == 0 || qDeg == 0) return cudaSuccess;
+    const uint32_t b = nBitsExt - nBits;
+    if (nBitsExt < nBits || nBitsExt > NTT_TWLG || (uint64_t)qDeg > (1ull << b)) return cudaErrorInvalidValue;
+    const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
+    cudaError_t err;
+    if (q_rowmajor) {
+        prof::Scope ps(prof::TRANSPOSE, stream);
+        dim3 grid((unsigned)((NExt + 31) / 32), (unsigned)((qDim + 31) / 32));
+        transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(d_scratch, d_q, NExt, qDim, NExt);
+        prof::count();
+    } else {
+        err = cudaMemcpyAsync(d_scratch, d_q, NExt * qDim * 8, cudaMemcpyDeviceToDevice, stream);
+        if (err != cudaSuccess) return err;
+    }
+    if ((err = cudaGetLastError()) != cudaSuccess) return err;
+    Window w[8];
+    const Tune tn = tuned(nBitsExt, nBitsExt, qDim);
+    int nw = plan_windows(0, nBitsExt, w, 8, tn.kfirst, tn.krest);
+    if (nw < 0) return cudaErrorInvalidValue;
+    {
+        prof::Scope ps(prof::NTT_INV, stream);
+        for (int i = nw - 1; i >= 0; i--) {
+            Pass p{};
+            p.src = d_scratch;
+            p.dst = d_scratch;
+            p.src_cs = p.dst_cs = NExt;
+            p.lg = nBitsExt;
+            p.s0 = w[i].s0;
+            p.k = w[i].k;
+            p.lgL = w[i].lgL;
+            p.dif = 1;
+            p.post = POST_NONE;
+            if ((err = launch_pass(p, qDim, stream)) != cudaSuccess) return err;
+        }
+    }
+    nw = plan_windows(b, nBitsExt, w, 8, tn.kfirst, tn.krest);
+    if (nw < 0) return cudaErrorInvalidValue;
+    prof::Scope ps(prof::NTT_FWD, stream);
+    const uint64_t shift_in = glh::pow(glh::inv(7), N), next_inv = glh::inv(NExt % GL_P);
+    uint64_t S = 1;
+    for (uint32_t pc = 0; pc < qDeg; pc++) {
+        Pass p{};
+        p.src = d_scratch;
+        p.dst = d_cmq + (uint64_t)pc * qDim * NExt;
+        p.src_cs = p.dst_cs = NExt;
+        p.lg = nBitsExt;
+        p.s0 = w[0].s0;
+        p.k = w[0].k;
+        p.lgL = w[0].lgL;
+        p.rep = b;
+        p.gshift = b;
+        uint64_t br = 0;
+        for (uint32_t t = 0; t < b; t++) br |= (uint64_t)((pc >> t) & 1) << (b - 1 - t);
+        p.goff = br;
+        p.scale = glh::mul(S, next_inv);  // nonzero: a product of nonzero field elements
+        p.post = (nw == 1) ? POST_CANON : POST_NONE;
+        if ((err = launch_pass(p, qDim, stream)) != cudaSuccess) return err;
+        S = glh::mul(S, shift_in);
+    }
+    for (int i = 1; i < nw; i++) {
+        Pass p{};
+        p.src = d_cmq;
+        p.dst = d_cmq;
+        p.src_cs = p.dst_cs = NExt;
+        p.lg = nBitsExt;
+        p.s0 = w[i].s0;
+        p.k = w[i].k;
+        p.lgL = w[i].lgL;
+        p.post = (i == nw - 1) ? POST_CANON : POST_NONE;
+        if ((err = launch_pass(p, (uint64_t)qDeg * qDim, stream)) != cudaSuccess) return err;
     }
     return cudaSuccess;
 }

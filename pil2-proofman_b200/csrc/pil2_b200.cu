@@ -51,6 +51,7 @@ static int ensure_init_current()
     CK(cudaFuncSetAttribute(ntt::pass16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (NTT_TILE_MAX + NTT_TILE_MAX / 16) * 8),
        "pass16_kernel smem attribute");
+    CK(ntt::set_fixed_attrs(), "pass_fixed_kernel smem attributes");
     g_init_done[dev] = true;
     return B200_OK;
 }
@@ -243,7 +244,7 @@ extern "C" const char *b200_kernel_names(void)
 {
     return "pass16_kernel\ntranspose_kernel\nleaf_hash_kernel\nnode_kernel\npermute_kernel\nlde_rows_kernel\n"
            "fill_kernel\nimad_probe_kernel\ntranspose_grouped\npass_grouped\nleaf_persistent\n"
-           "node_grouped\ngather_roots\n";
+           "node_grouped\ngather_roots\npass_fixed_kernel\n";
 }
 
 // ------------------------------------------------------------ host-buffer API ----
