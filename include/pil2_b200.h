@@ -259,6 +259,51 @@ uint64_t b200_launch_count(void);
  * mad.lo/mad.hi chains of `iters` steps; returns the measured rate in G IMAD/s. */
 int b200_probe_imad(uint64_t blocks, uint64_t iters, double *gimad_per_s);
 
+/* ---- FRI query openings from the resident LDE and tree ----
+ * One opening = MerkleTreeGL::getGroupProof (merkleTreeGL.cpp:145-175): the row's nCols values,
+ * then per tree level the (arity-1) sibling digests of the path node in child order, up to the
+ * root, or with last_level_verification = llv > 0 until a level holds <= arity^llv nodes.
+ * Replaces the GPU reference's getTreeTracePols + genMerkleProof (starks_gpu.cu:903-1042).
+ * d_lde column-major NExt x nCols, d_tree in the reference layout, d_rows nQueries row indices;
+ * d_out receives nQueries x b200_query_proof_words() words. */
+uint64_t b200_query_proof_words(uint64_t NExt, uint64_t nCols, uint64_t arity, uint64_t last_level_verification);
+int b200_query_openings_device(uint64_t *d_out, const uint64_t *d_lde, uint64_t NExt, uint64_t nCols,
+                               const uint64_t *d_tree, uint64_t arity, uint64_t last_level_verification,
+                               const uint64_t *d_rows, uint64_t nQueries, void *stream);
+
+/* ---- Q-stage commit (Starks::computeQ, starks.hpp:186-239; computeQColMajor,
+ * ntt_goldilocks.cu:1515-1544) ----
+ * d_q: qDim limb columns of NExt quotient evaluations (column-major, or row-major NExt x qDim);
+ * d_cmq: column-major NExt x (qDeg*qDim), column p*qDim + k = chunk p of limb k extended;
+ * d_tree: b200_tree_num_elements(NExt, arity) words; d_scratch: b200_q_scratch_words() words.
+ * Requires qDeg <= NExt / N.  root_host (optional) receives the root after a stream sync. */
+uint64_t b200_q_scratch_words(uint64_t nBitsExt, uint64_t qDim);
+int b200_commit_q_device(uint64_t *root_host, uint64_t *d_cmq, uint64_t *d_tree, const uint64_t *d_q,
+                         int q_rowmajor, uint64_t nBits, uint64_t nBitsExt, uint64_t qDeg, uint64_t qDim,
+                         uint64_t arity, uint64_t *d_scratch, void *stream);
+
+/* ---- LDE plan autotuner (no reference counterpart: the reference's NTT has a fixed plan) ----
+ * b200_autotune_lde times the LDE of (nBits, nBitsExt) under each window plan on a probe of
+ * min(nCols, 64) columns and records the fastest for nCols' bucket; plain, batched and served
+ * commits then use it.  Plans change speed only, never results.  The table can be read, set,
+ * saved to and loaded from a text file. */
+int b200_autotune_lde(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, double *best_ms, uint32_t *kfirst,
+                      uint32_t *krest);
+void b200_autotune_get(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint32_t *kfirst, uint32_t *krest);
+void b200_autotune_set(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint32_t kfirst, uint32_t krest);
+int b200_autotune_save(const char *path);
+int b200_autotune_load(const char *path);
+
+/* ---- packed-witness commit (PackedInfo + unpack, starks_gpu.cu:49-103; the packed branch of
+ * commit_witness_gpu, starks_api.cu:1660-1676) ----
+ * d_packed: N rows of words_per_row u64 words; column c takes the next col_bits[c] (1..64) bits
+ * of its row, least significant first, straddling words.  col_bits is a host array.  Same
+ * outputs as b200_commit_device on the unpacked trace. */
+uint64_t b200_packed_words_per_row(const uint32_t *col_bits, uint64_t nCols);
+int b200_commit_packed_device(uint64_t *root_host, uint64_t *d_lde, uint64_t *d_tree, const uint64_t *d_packed,
+                              uint64_t words_per_row, const uint32_t *col_bits, uint64_t nBits, uint64_t nBitsExt,
+                              uint64_t nCols, uint64_t arity, uint64_t *d_scratch, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -102,6 +102,9 @@ class Oracle(_Base):
             "orc_tree_num_elements": [_u64, _u64],
             "orc_root_of_unity": [ctypes.c_uint],
             "orc_set_hash_family": [ctypes.c_int],
+            "orc_group_proof": [_vp, _vp, _u64, _u64, _vp, _u64, _u64, _u64],
+            "orc_root_from_proof": [_vp, _vp, _u64, _u64, _u64, _u64],
+            "orc_commit_q": [_vp, _vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64],
             "orc_p1_permute": [ctypes.c_uint, _vp],
             "orc_merkletree_w": [ctypes.c_uint, _vp, _vp, _u64, _u64, _u64],
             "orc_mul": [_u64, _u64],
@@ -110,9 +113,11 @@ class Oracle(_Base):
         }.items():
             f = getattr(lib, name)
             f.argtypes = args
-        for name in ("orc_tree_num_elements", "orc_root_of_unity", "orc_mul", "orc_add", "orc_sub"):
+        for name in ("orc_tree_num_elements", "orc_root_of_unity", "orc_mul", "orc_add", "orc_sub",
+                     "orc_group_proof"):
             getattr(lib, name).restype = _u64
-        for name in ("orc_merkletree_w", "orc_merkletree", "orc_merkletree_colmajor", "orc_merkletree_reduce"):
+        for name in ("orc_merkletree_w", "orc_merkletree", "orc_merkletree_colmajor", "orc_merkletree_reduce",
+                     "orc_commit_q"):
             getattr(lib, name).restype = ctypes.c_int
         self.lib = lib
 
@@ -176,6 +181,34 @@ class Oracle(_Base):
         if self.lib.orc_merkletree_reduce(width, _ptr(root), _ptr(digests), digests.size // 4, arity) != 0:
             raise ValueError("width must be 4*arity")
         return root
+
+    def group_proof(self, lde_rowmajor, tree, arity, row, llv=0):
+        """MerkleTreeGL::getGroupProof of one row (row values + sibling digests)."""
+        lde_rowmajor = np.ascontiguousarray(lde_rowmajor, dtype=np.uint64)
+        tree = np.ascontiguousarray(tree, dtype=np.uint64)
+        nrows, ncols = lde_rowmajor.shape
+        out = np.zeros(ncols + 64 * 3 * 4, dtype=np.uint64)
+        n = self.lib.orc_group_proof(_ptr(out), _ptr(lde_rowmajor), nrows, ncols, _ptr(tree), arity, llv, row)
+        return out[:n].copy()
+
+    def root_from_proof(self, proof, ncols, nrows, arity, row):
+        proof = np.ascontiguousarray(proof, dtype=np.uint64)
+        root = np.zeros(4, dtype=np.uint64)
+        self._fam()
+        self.lib.orc_root_from_proof(_ptr(root), _ptr(proof), ncols, nrows, arity, row)
+        return root
+
+    def commit_q(self, q, nbits, nbits_ext, qdeg, qdim, arity):
+        """Starks::computeQ restated: q row-major (NExt, qDim) -> (root, cmQ row-major, tree)."""
+        q = np.ascontiguousarray(q, dtype=np.uint64)
+        next_ = 1 << nbits_ext
+        root = np.zeros(4, dtype=np.uint64)
+        cmq = np.zeros((next_, qdeg * qdim), dtype=np.uint64)
+        tree = np.zeros(tree_num_elements(next_, arity), dtype=np.uint64)
+        self._fam()
+        if self.lib.orc_commit_q(_ptr(root), _ptr(cmq), _ptr(tree), _ptr(q), nbits, nbits_ext, qdeg, qdim, arity):
+            raise ValueError("bad Q shape")
+        return root, cmq, tree
 
     def root_of_unity(self, k):
         return int(self.lib.orc_root_of_unity(k))

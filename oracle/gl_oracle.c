@@ -444,3 +444,98 @@ int orc_commit(uint64_t root[4], uint64_t *lde, uint64_t *tree, const uint64_t *
     if (!tree) free(t);
     return rc;
 }
+
+/* ------------------------------------------------------ query openings ---- */
+
+static uint64_t ipow_u(uint64_t b, uint64_t e)
+{
+    uint64_t r = 1;
+    while (e--) r *= b;
+    return r;
+}
+
+/* MerkleTreeGL::getGroupProof (merkleTreeGL.cpp:145-175): the row's ncols words, then per level
+ * the (arity-1) sibling digests of the path node in child order, until the root or until a level
+ * has <= arity^llv nodes.  lde is row-major nrows x ncols; returns the number of words written. */
+uint64_t orc_group_proof(uint64_t *out, const uint64_t *lde, uint64_t nrows, uint64_t ncols, const uint64_t *tree,
+                         uint64_t arity, uint64_t llv, uint64_t row)
+{
+    uint64_t w = 0;
+    for (uint64_t c = 0; c < ncols; c++) out[w++] = canon(lde[row * ncols + c]);
+    uint64_t idx = row, offset = 0, n = nrows;
+    const uint64_t stop = llv ? ipow_u(arity, llv) : 1;
+    while (llv ? (n > stop) : (n > 1)) {
+        const uint64_t cur = idx % arity, si = idx - cur;
+        for (uint64_t i = 0; i < arity; i++) {
+            if (i == cur) continue;
+            for (int j = 0; j < 4; j++) out[w++] = tree[(offset + si + i) * 4 + j];
+        }
+        const uint64_t next = (n + arity - 1) / arity;
+        offset += next * arity;
+        idx /= arity;
+        n = next;
+    }
+    return w;
+}
+
+/* Recompute the root (llv = 0) from an opening: leaf = linear hash of the row, then one
+ * permutation per level over the arity children with the path node at its position
+ * (MerkleTreeGL::verifyGroupProof / calculateRootFromProof, merkleTreeGL.cpp:177-296). */
+void orc_root_from_proof(uint64_t root[4], const uint64_t *proof, uint64_t ncols, uint64_t nrows, uint64_t arity,
+                         uint64_t row)
+{
+    unsigned w = (unsigned)(4 * arity);
+    uint64_t h[4];
+    linear_hash_strided(w, h, proof, 1, ncols);
+    const uint64_t *sib = proof + ncols;
+    uint64_t idx = row, n = nrows;
+    while (n > 1) {
+        const uint64_t cur = idx % arity;
+        uint64_t st[16];
+        unsigned p = 0;
+        for (uint64_t i = 0; i < arity; i++) {
+            const uint64_t *src = (i == cur) ? h : sib + 4 * (p++);
+            memcpy(st + 4 * i, src, 32);
+        }
+        sib += 4 * (arity - 1);
+        permute_fam(w, st);
+        memcpy(h, st, 32);
+        idx /= arity;
+        n = (n + arity - 1) / arity;
+    }
+    memcpy(root, h, 32);
+}
+
+/* ------------------------------------------------------------ Q-stage commit ---- */
+
+/* Starks::computeQ (starks.hpp:186-239): q is row-major NExt x qDim (evaluations); each limb
+ * column is inverse-transformed over NExt; coefficient p*N + i of limb k, times
+ * S[p] = (7^-1)^(N*p), becomes row i of cmQ column p*qDim + k (rows N..NExt-1 zero); each cmQ
+ * column is forward-transformed over NExt; then the Merkle tree of cmQ (row-major NExt x
+ * qDeg*qDim).  cmq and tree may be NULL. */
+int orc_commit_q(uint64_t root[4], uint64_t *cmq, uint64_t *tree, const uint64_t *q, uint64_t nBits, uint64_t nBitsExt,
+                 uint64_t qDeg, uint64_t qDim, uint64_t arity)
+{
+    const uint64_t N = 1ULL << nBits, NExt = 1ULL << nBitsExt, ncols = qDeg * qDim;
+    if (nBitsExt < nBits || qDeg * N > NExt || arity < 2 || arity > 4) return -1;
+    uint64_t *coef = (uint64_t *)malloc(NExt * qDim * sizeof(uint64_t));
+    orc_ntt(coef, q, NExt, qDim, 1);
+    uint64_t *cm = cmq ? cmq : (uint64_t *)malloc(NExt * ncols * sizeof(uint64_t));
+    memset(cm, 0, NExt * ncols * sizeof(uint64_t));
+    const uint64_t shift_in = gl_pow(gl_inv(7), N);
+    uint64_t S = 1;
+    for (uint64_t p = 0; p < qDeg; p++) {
+        for (uint64_t i = 0; i < N; i++)
+            for (uint64_t k = 0; k < qDim; k++) cm[i * ncols + p * qDim + k] = gl_mul(coef[(p * N + i) * qDim + k], S);
+        S = gl_mul(S, shift_in);
+    }
+    free(coef);
+    orc_ntt(cm, cm, NExt, ncols, 0);
+    const uint64_t total = orc_tree_num_elements(NExt, arity);
+    uint64_t *t = tree ? tree : (uint64_t *)malloc(total * sizeof(uint64_t));
+    int rc = orc_merkletree(t, cm, ncols, NExt, arity);
+    memcpy(root, t + total - 4, 4 * sizeof(uint64_t));
+    if (!cmq) free(cm);
+    if (!tree) free(t);
+    return rc;
+}

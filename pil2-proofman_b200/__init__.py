@@ -82,6 +82,19 @@ _SIGS = {
     "b200_server_release": (_i32, [_vp, ctypes.c_int64]),
     "b200_server_buffers": (_i32, [_vp, ctypes.c_int64, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "b200_server_free": (None, [_vp]),
+    # query openings, Q stage, plan autotuner, packed witness
+    "b200_query_proof_words": (_u64, [_u64, _u64, _u64, _u64]),
+    "b200_query_openings_device": (_i32, [_vp, _vp, _u64, _u64, _vp, _u64, _u64, _vp, _u64, _vp]),
+    "b200_q_scratch_words": (_u64, [_u64, _u64]),
+    "b200_commit_q_device": (_i32, [_vp, _vp, _vp, _vp, _i32, _u64, _u64, _u64, _u64, _u64, _vp, _vp]),
+    "b200_autotune_lde": (_i32, [_u64, _u64, _u64, ctypes.POINTER(ctypes.c_double),
+                                 ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
+    "b200_autotune_get": (None, [_u64, _u64, _u64, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
+    "b200_autotune_set": (None, [_u64, _u64, _u64, ctypes.c_uint32, ctypes.c_uint32]),
+    "b200_autotune_save": (_i32, [ctypes.c_char_p]),
+    "b200_autotune_load": (_i32, [ctypes.c_char_p]),
+    "b200_packed_words_per_row": (_u64, [_vp, _u64]),
+    "b200_commit_packed_device": (_i32, [_vp, _vp, _vp, _vp, _u64, _vp, _u64, _u64, _u64, _u64, _vp, _vp]),
 }
 
 _lib = None
@@ -307,3 +320,89 @@ def probe_imad(blocks=148 * 16, iters=1 << 16):
     _check(load().b200_probe_imad(blocks, iters, ctypes.byref(r)))
     return r.value
 
+
+
+# ---------------------------------------------------------------- query openings ----
+def query_proof_words(next_, ncols, arity, llv=0):
+    """Words of one opening (MerkleTreeGL::getGroupProof layout)."""
+    return int(load().b200_query_proof_words(next_, ncols, arity, llv))
+
+
+def query_openings_device(d_out, d_lde, next_, ncols, d_tree, arity, d_rows, nqueries, llv=0, stream=None):
+    _check(load().b200_query_openings_device(_ptr(d_out), _ptr(d_lde), next_, ncols, _ptr(d_tree), arity, llv,
+                                             _ptr(d_rows), nqueries, _stream(stream)))
+
+
+# ---------------------------------------------------------------- Q stage ----
+def q_scratch_words(nbits_ext, qdim):
+    return int(load().b200_q_scratch_words(nbits_ext, qdim))
+
+
+def commit_q_device(d_cmq, d_tree, d_q, nbits, nbits_ext, qdeg, qdim, arity, d_scratch, q_rowmajor=True,
+                    stream=None):
+    root = np.zeros(4, dtype=np.uint64)
+    _check(load().b200_commit_q_device(_ptr(root), _ptr(d_cmq), _ptr(d_tree), _ptr(d_q), 1 if q_rowmajor else 0,
+                                       nbits, nbits_ext, qdeg, qdim, arity, _ptr(d_scratch), _stream(stream)))
+    return root
+
+
+# ---------------------------------------------------------------- plan autotuner ----
+def autotune_lde(nbits, nbits_ext, ncols):
+    """Time every window plan for this shape; returns (best ms on the probe, kfirst, krest)."""
+    ms, kf, kr = ctypes.c_double(), ctypes.c_uint32(), ctypes.c_uint32()
+    _check(load().b200_autotune_lde(nbits, nbits_ext, ncols, ctypes.byref(ms), ctypes.byref(kf), ctypes.byref(kr)))
+    return ms.value, kf.value, kr.value
+
+
+def autotune_get(nbits, nbits_ext, ncols):
+    kf, kr = ctypes.c_uint32(), ctypes.c_uint32()
+    load().b200_autotune_get(nbits, nbits_ext, ncols, ctypes.byref(kf), ctypes.byref(kr))
+    return kf.value, kr.value
+
+
+def autotune_set(nbits, nbits_ext, ncols, kfirst, krest):
+    load().b200_autotune_set(nbits, nbits_ext, ncols, kfirst, krest)
+
+
+def autotune_save(path):
+    _check(load().b200_autotune_save(path.encode()))
+
+
+def autotune_load(path):
+    _check(load().b200_autotune_load(path.encode()))
+
+
+# ---------------------------------------------------------------- packed witness ----
+def packed_words_per_row(col_bits):
+    bits = np.ascontiguousarray(col_bits, dtype=np.uint32)
+    return int(load().b200_packed_words_per_row(bits.ctypes.data, bits.size))
+
+
+def commit_packed_device(d_lde, d_tree, d_packed, words_per_row, col_bits, nbits, nbits_ext, arity, d_scratch,
+                         stream=None):
+    bits = np.ascontiguousarray(col_bits, dtype=np.uint32)
+    root = np.zeros(4, dtype=np.uint64)
+    _check(load().b200_commit_packed_device(_ptr(root), _ptr(d_lde), _ptr(d_tree), _ptr(d_packed), words_per_row,
+                                            bits.ctypes.data if bits.size else None, nbits, nbits_ext, bits.size,
+                                            arity, _ptr(d_scratch), _stream(stream)))
+    return root
+
+
+def pack_rows(trace, col_bits):
+    """Host packer (row-major trace, per-column widths) -> (N, words_per_row) uint64: the inverse of the
+    device unpack, used by tests and benchmarks to build packed witnesses."""
+    trace = np.ascontiguousarray(trace, dtype=np.uint64)
+    n, ncols = trace.shape
+    bits = [int(b) for b in col_bits]
+    wpr = (sum(bits) + 63) // 64
+    out = np.zeros((n, wpr), dtype=np.uint64)
+    off = 0
+    for c, nb in enumerate(bits):
+        mask = np.uint64((1 << nb) - 1) if nb < 64 else np.uint64(0xFFFFFFFFFFFFFFFF)
+        v = trace[:, c] & mask
+        w, o = divmod(off, 64)
+        out[:, w] |= v << np.uint64(o)
+        if o + nb > 64:
+            out[:, w + 1] |= v >> np.uint64(64 - o)
+        off += nb
+    return out

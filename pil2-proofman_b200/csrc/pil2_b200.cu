@@ -244,7 +244,7 @@ extern "C" const char *b200_kernel_names(void)
 {
     return "pass16_kernel\ntranspose_kernel\nleaf_hash_kernel\nnode_kernel\npermute_kernel\nlde_rows_kernel\n"
            "fill_kernel\nimad_probe_kernel\ntranspose_grouped\npass_grouped\nleaf_persistent\n"
-           "node_grouped\ngather_roots\npass_fixed_kernel\n";
+           "node_grouped\ngather_roots\npass_fixed_kernel\nopenings_kernel\nunpack_kernel\n";
 }
 
 // ------------------------------------------------------------ host-buffer API ----
@@ -707,3 +707,214 @@ extern "C" int b200_probe_imad(uint64_t blocks, uint64_t iters, double *gimad_pe
 // ---------------------------------------------------- batched commit and server ----
 #include "batch_api.cuh"
 #include "server.cuh"
+
+// ------------------------------------------------------------- query openings ----
+#include "query.cuh"
+
+extern "C" uint64_t b200_query_proof_words(uint64_t NExt, uint64_t nCols, uint64_t arity,
+                                           uint64_t last_level_verification)
+{
+    if (arity < 2 || arity > 4 || NExt == 0) return 0;
+    return query::proof_words(NExt, nCols, arity, last_level_verification);
+}
+
+extern "C" int b200_query_openings_device(uint64_t *d_out, const uint64_t *d_lde, uint64_t NExt, uint64_t nCols,
+                                          const uint64_t *d_tree, uint64_t arity, uint64_t last_level_verification,
+                                          const uint64_t *d_rows, uint64_t nQueries, void *stream)
+{
+    if (arity < 2 || arity > 4) return set_err(B200_EINVAL, "arity must be 2, 3 or 4");
+    if (NExt == 0) return set_err(B200_EINVAL, "empty tree");
+    if (nQueries == 0) return B200_OK;
+    if (nQueries > 0x7fffffffULL) return set_err(B200_EINVAL, "too many queries");
+    if (!d_out || !d_tree || !d_rows || (nCols && !d_lde)) return set_err(B200_EINVAL, "null buffer");
+    const uint64_t levels = query::proof_levels(NExt, arity, last_level_verification);
+    const uint64_t words = nCols + levels * (arity - 1) * 4;
+    query::openings_kernel<<<(unsigned)nQueries, 256, 0, (cudaStream_t)stream>>>(d_out, d_lde, NExt, nCols, d_tree,
+                                                                                 arity, levels, d_rows, words);
+    CK(cudaGetLastError(), "query openings");
+    return B200_OK;
+}
+
+// ------------------------------------------------------------ Q-stage commit ----
+extern "C" uint64_t b200_q_scratch_words(uint64_t nBitsExt, uint64_t qDim) { return (1ull << nBitsExt) * qDim; }
+
+extern "C" int b200_commit_q_device(uint64_t *root_host, uint64_t *d_cmq, uint64_t *d_tree, const uint64_t *d_q,
+                                    int q_rowmajor, uint64_t nBits, uint64_t nBitsExt, uint64_t qDeg, uint64_t qDim,
+                                    uint64_t arity, uint64_t *d_scratch, void *stream)
+{
+    int rc = check_shape(nBits, nBitsExt, qDeg * qDim, arity);
+    if (rc) return rc;
+    if (qDeg > (1ull << (nBitsExt - nBits))) return set_err(B200_EINVAL, "qDeg above NExt / N");
+    if ((rc = ensure_init_current())) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint64_t NExt = 1ull << nBitsExt, ncols = qDeg * qDim;
+    if (!d_tree || (ncols && (!d_cmq || !d_q || !d_scratch))) return set_err(B200_EINVAL, "null buffer");
+    CK(ntt::lde_q(d_cmq, d_q, q_rowmajor != 0, (uint32_t)nBits, (uint32_t)nBitsExt, (uint32_t)qDeg, (uint32_t)qDim,
+                  d_scratch, s),
+       "Q extension");
+    CK(merkle::build_tree_arity(arity, d_tree, d_cmq, 1, NExt, ncols, NExt, s), "merkletree");
+    if (root_host) {
+        const uint64_t total = merkle::tree_num_elements(NExt, arity);
+        CK(cudaMemcpyAsync(root_host, d_tree + total - 4, 32, cudaMemcpyDeviceToHost, s), "root D2H");
+        CK(cudaStreamSynchronize(s), "sync");
+    }
+    return B200_OK;
+}
+
+// ------------------------------------------------------------ plan autotuner ----
+// Times lde() under each candidate plan (largest first window kf, largest later window kr,
+// both in 8..12) on a probe of min(nCols, 64) columns of seeded data, and keeps the fastest for
+// the shape's column bucket.  Untimed set-up for callers; every plan computes the same values.
+extern "C" int b200_autotune_lde(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, double *best_ms,
+                                 uint32_t *kfirst, uint32_t *krest)
+{
+    int rc = check_shape(nBits, nBitsExt, nCols, 4);
+    if (rc) return rc;
+    if ((rc = ensure_init_current())) return rc;
+    const uint64_t probe = nCols < 64 ? (nCols ? nCols : 1) : 64;
+    const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
+    uint64_t *d_trace = nullptr, *d_lde = nullptr, *d_scr = nullptr;
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    auto cleanup = [&]() {
+        if (d_trace) cudaFree(d_trace);
+        if (d_lde) cudaFree(d_lde);
+        if (d_scr) cudaFree(d_scr);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (s) cudaStreamDestroy(s);
+    };
+    if (cudaMalloc(&d_trace, N * probe * 8) != cudaSuccess || cudaMalloc(&d_lde, NExt * probe * 8) != cudaSuccess ||
+        cudaMalloc(&d_scr, N * probe * 8) != cudaSuccess || cudaStreamCreate(&s) != cudaSuccess ||
+        cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        cleanup();
+        cudaGetLastError();
+        return set_err(B200_ENOMEM, "autotune buffers");
+    }
+    synth::fill_kernel<<<(unsigned)((N * probe + 255) / 256), 256, 0, s>>>(d_trace, N * probe, 99);
+    double best = 1e30;
+    ntt::Tune bt{};
+    for (uint32_t kf = 8; kf <= NTT_KMAX; kf++) {
+        for (uint32_t kr = 8; kr <= NTT_KMAX; kr++) {
+            ntt::set_tuned((uint32_t)nBits, (uint32_t)nBitsExt, nCols, ntt::Tune{kf, kr});
+            // one warm-up, then the best of three
+            float ms_best = 1e30f;
+            bool ok = true;
+            for (int it = 0; it < 4 && ok; it++) {
+                cudaEventRecord(e0, s);
+                ok = ntt::lde(d_lde, d_trace, true, (uint32_t)nBits, (uint32_t)nBitsExt, probe, d_scr, s) ==
+                     cudaSuccess;
+                cudaEventRecord(e1, s);
+                float ms = 0;
+                if (ok) ok = cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+                if (it > 0 && ms < ms_best) ms_best = ms;
+            }
+            if (!ok) {
+                cleanup();
+                return set_err(B200_ECUDA, "autotune run failed");
+            }
+            if (ms_best < best) {
+                best = ms_best;
+                bt = ntt::Tune{kf, kr};
+            }
+        }
+    }
+    ntt::set_tuned((uint32_t)nBits, (uint32_t)nBitsExt, nCols, bt);
+    cleanup();
+    if (best_ms) *best_ms = best;
+    if (kfirst) *kfirst = bt.kfirst;
+    if (krest) *krest = bt.krest;
+    return B200_OK;
+}
+
+extern "C" void b200_autotune_get(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint32_t *kfirst,
+                                  uint32_t *krest)
+{
+    const ntt::Tune t = ntt::tuned((uint32_t)nBits, (uint32_t)nBitsExt, nCols);
+    if (kfirst) *kfirst = t.kfirst;
+    if (krest) *krest = t.krest;
+}
+
+extern "C" void b200_autotune_set(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint32_t kfirst, uint32_t krest)
+{
+    ntt::set_tuned((uint32_t)nBits, (uint32_t)nBitsExt, nCols, ntt::Tune{kfirst, krest});
+}
+
+// table file: one line per tuned key, "key kfirst krest"
+extern "C" int b200_autotune_save(const char *path)
+{
+    std::lock_guard<std::mutex> lk(ntt::tune_mu());
+    std::ofstream f(path);
+    if (!f) return set_err(B200_EINVAL, "cannot open plan file for writing");
+    for (const auto &kv : ntt::tune_table()) f << kv.first << " " << kv.second.kfirst << " " << kv.second.krest << "\n";
+    return f ? B200_OK : set_err(B200_EINVAL, "plan file write failed");
+}
+
+extern "C" int b200_autotune_load(const char *path)
+{
+    std::ifstream f(path);
+    if (!f) return set_err(B200_EINVAL, "cannot open plan file");
+    uint64_t key;
+    uint32_t kf, kr;
+    std::lock_guard<std::mutex> lk(ntt::tune_mu());
+    while (f >> key >> kf >> kr) {
+        if (kf < 1 || kf > NTT_KMAX || kr < 1 || kr > NTT_KMAX) return set_err(B200_EINVAL, "bad plan entry");
+        ntt::tune_table()[key] = ntt::Tune{kf, kr};
+    }
+    return B200_OK;
+}
+
+// ------------------------------------------------------ packed-witness commit ----
+#include "unpack.cuh"
+
+extern "C" uint64_t b200_packed_words_per_row(const uint32_t *col_bits, uint64_t nCols)
+{
+    return (unpack::packed_bits(col_bits, nCols) + 63) / 64;
+}
+
+// Commit of a bit-packed row-major witness (the reference's packed trace: PackedInfo and the
+// unpack kernel, starks_gpu.cu:49-103; commit_witness_gpu's packed branch, starks_api.cu:1660-1676):
+// the packed rows are unpacked straight into the column-major scratch, which the LDE then
+// transforms in place.  col_bits: host array of nCols widths in 1..64; d_packed: N x
+// words_per_row words with words_per_row = b200_packed_words_per_row(col_bits, nCols).
+extern "C" int b200_commit_packed_device(uint64_t *root_host, uint64_t *d_lde, uint64_t *d_tree,
+                                         const uint64_t *d_packed, uint64_t words_per_row, const uint32_t *col_bits,
+                                         uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t arity,
+                                         uint64_t *d_scratch, void *stream)
+{
+    int rc = check_shape(nBits, nBitsExt, nCols, arity);
+    if (rc) return rc;
+    if (nCols && !col_bits) return set_err(B200_EINVAL, "null column widths");
+    for (uint64_t c = 0; c < nCols; c++)
+        if (col_bits[c] < 1 || col_bits[c] > 64) return set_err(B200_EINVAL, "column width outside 1..64");
+    if (nCols > 12288) return set_err(B200_EINVAL, "packed commit supports at most 12288 columns");
+    if (nCols && words_per_row * 64 < unpack::packed_bits(col_bits, nCols))
+        return set_err(B200_EINVAL, "words_per_row too small for the column widths");
+    if ((rc = ensure_init_current())) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
+    if (!d_tree || (nCols && (!d_lde || !d_packed || !d_scratch))) return set_err(B200_EINVAL, "null buffer");
+    if (nCols) {
+        uint32_t *d_bits = nullptr;
+        CK(cudaMallocAsync((void **)&d_bits, nCols * 4, s), "column widths buffer");
+        CK(cudaMemcpyAsync(d_bits, col_bits, nCols * 4, cudaMemcpyHostToDevice, s), "column widths H2D");
+        {
+            prof::Scope ps(prof::TRANSPOSE, s);
+            unpack::unpack_kernel<<<(unsigned)((N + 255) / 256), 256, nCols * 4, s>>>(d_scratch, d_packed, N, nCols,
+                                                                                     words_per_row, d_bits);
+            prof::count();
+        }
+        const cudaError_t e = cudaGetLastError();
+        cudaFreeAsync(d_bits, s);
+        CK(e, "unpack");
+        // the trace now sits column-major in the scratch; the LDE transforms it in place
+        CK(ntt::lde(d_lde, d_scratch, false, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, d_scratch, s), "lde");
+    }
+    CK(merkle::build_tree_arity(arity, d_tree, d_lde, 1, NExt, nCols, NExt, s), "merkletree");
+    if (root_host) {
+        const uint64_t total = merkle::tree_num_elements(NExt, arity);
+        CK(cudaMemcpyAsync(root_host, d_tree + total - 4, 32, cudaMemcpyDeviceToHost, s), "root D2H");
+        CK(cudaStreamSynchronize(s), "sync");
+    }
+    return B200_OK;
+}

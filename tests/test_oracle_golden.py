@@ -200,3 +200,35 @@ def test_p1_oracle_matches_reference_build(orc1):
     m = oracle.random_field((100, 9), 7)
     for w, arity in ((8, 2), (12, 2), (12, 3), (16, 2), (16, 3), (16, 4)):
         assert (orc1.merkletree_w(w, m, arity) == ref1.merkletree_w(w, m, arity)).all(), (w, arity)
+
+
+@pytest.mark.parametrize("family", [1, 2])
+@pytest.mark.parametrize("arity", [2, 3, 4])
+def test_group_proof_roundtrip(family, arity):
+    """Oracle openings hash back to the root (both hash families); llv > 0 stops early."""
+    o = oracle.Oracle(family=family)
+    m = oracle.random_field((200, 9), 31 + arity)
+    tree = o.merkletree(m, arity)
+    for row in (0, 57, 199):
+        proof = o.group_proof(m, tree, arity, row)
+        assert (o.root_from_proof(proof, 9, 200, arity, row) == tree[-4:]).all()
+        short = o.group_proof(m, tree, arity, row, llv=2)
+        assert len(short) < len(proof) and (short == proof[:len(short)]).all()
+
+
+def test_commit_q_coefficient_chunks(orc):
+    """computeQ restated: chunk p of each limb's coefficients, times (7^-1)^(N*p), is column
+    p*qDim + k of cmQ, which has degree < N."""
+    nb, nbe, qdeg, qdim = 4, 6, 3, 3
+    q = oracle.random_field((1 << nbe, qdim), 5)
+    _, cmq, _ = orc.commit_q(q, nb, nbe, qdeg, qdim, 4)
+    co = orc.ntt(cmq, inverse=True)
+    assert not co[1 << nb:].any()
+    qc = orc.ntt(q, inverse=True)
+    P = oracle.P
+    shift_in = pow(pow(7, P - 2, P), 1 << nb, P)
+    for p in range(qdeg):
+        S = pow(shift_in, p, P)
+        for i in range(1 << nb):
+            for k in range(qdim):
+                assert int(co[i, p * qdim + k]) == int(qc[p * (1 << nb) + i, k]) * S % P
