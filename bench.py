@@ -36,6 +36,10 @@ WORKLOADS = {
                nbits=22, nbits_ext=23, ncols=256, arity=4, sample_nbits=17),
     "c1": dict(desc="single AIR 2^16 x 32 base columns, blowup 2, Poseidon2 W16 arity-4 tree",
                nbits=16, nbits_ext=17, ncols=32, arity=4, sample_nbits=16),
+    # stage-2-style commit: 600 base + 60 cubic-extension columns (3 limbs each, hashed in row-major
+    # limb order) = 780 words per row, blowup 4 (LDE 2^22 rows, 26 GB)
+    "c4": dict(desc="stage-2 AIR 2^20 x (600 base + 60 cubic = 780 limbs), blowup 4, Poseidon2 W16 arity-4 tree",
+               nbits=20, nbits_ext=22, ncols=780, arity=4, sample_nbits=14),
     # profiling case of the 256-column workload: LDE 2.1 GB (larger than L2), ~4.3 GB on the device
     "c2s": dict(desc="single AIR 2^19 x 256 base columns, blowup 2, Poseidon2 W16 arity-4 tree",
                 nbits=19, nbits_ext=20, ncols=256, arity=4, sample_nbits=16),
@@ -231,6 +235,11 @@ def run_ours(args, wl):
     lde = torch.empty(elems, dtype=torch.int64, device=dev)
     tree = torch.empty(pkg.tree_num_elements(NExt, arity), dtype=torch.int64, device=dev)
     pkg.fill_random_device(trace, N * ncols, 1000 + rank, stream)
+    tuned = None
+    if not args.no_autotune:  # untimed set-up: pick the NTT window plan for this shape
+        t_ms, kf, kr = pkg.autotune_lde(nbits, nbe, ncols)
+        tuned = {"kfirst": kf, "krest": kr, "probe_ms": round(t_ms, 3)}
+    args.tuned_plan = tuned
     roots = []
     for _ in range(args.warmup):
         roots.append(pkg.commit_device(lde, tree, trace, nbits, nbe, ncols, arity, scratch, stream=stream))
@@ -339,6 +348,7 @@ def finish(args, wl, pkg, dist, rank, world, value, ms, launches, kernel_ms, roo
         "e2e": e2e_obj,
         "gpu_launches": int(launches),
         "kernel_ms_per_step": kernel_ms,
+        "ntt_plan": getattr(args, "tuned_plan", None) or "default (autotuner off)",
         "roofline": roofline,
         "clocks": clocks,
         "root": [hex(int(v)) for v in roots[0]] if rank == 0 else None,
@@ -366,6 +376,23 @@ def c3_shapes(seed=3, n=64):
     return [(int(a), int(a + b), int(c)) for a, b, c in zip(nbits, blow, ncols)]
 
 
+def c3small_shapes(seed=4, n=256):
+    """256 small AIR instances: log2 rows uniform in 10..16, columns uniform in [8, 128], blowup 2
+    for three quarters and 4 for a quarter: the regime where per-instance launches dominate."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nbits = rng.integers(10, 17, size=n)
+    ncols = rng.integers(8, 129, size=n)
+    blow = np.array([1] * (3 * n // 4) + [2] * (n - 3 * n // 4))
+    rng.shuffle(blow)
+    return [(int(a), int(a + b), int(c)) for a, b, c in zip(nbits, blow, ncols)]
+
+
+BATCH_SETS = {
+    "c3": (c3_shapes, "64 AIR instances, log2 rows U{16..22}, cols U[16,512], blowup 2 (48) / 4 (16)"),
+    "c3small": (c3small_shapes, "256 AIR instances, log2 rows U{10..16}, cols U[8,128], blowup 2 (3/4) / 4 (1/4)"),
+}
+
+
 def instance_words(pkg, nb, nbe, nc, arity=4):
     N, NExt = 1 << nb, 1 << nbe
     return N * nc, N * nc, NExt * nc, pkg.tree_num_elements(NExt, arity)
@@ -380,7 +407,8 @@ def run_batched(args):
     pkg.init(0)
     lib = pkg.load()
     dev = torch.device("cuda", 0)
-    shapes = c3_shapes()
+    make_shapes, shapes_desc = BATCH_SETS[args.workload]
+    shapes = make_shapes()
     budget = int(args.budget_gb * 2**30) // 8  # words
     waves, cur, used = [], [], 0
     for i, (nb, nbe, nc) in enumerate(shapes):
@@ -449,7 +477,7 @@ def run_batched(args):
         del arena
         torch.cuda.empty_cache()
     line = {
-        "metric": METRIC + " - batched vs plain", "workload": "c3",
+        "metric": METRIC + " - batched vs plain", "workload": args.workload,
         "value": round(total_elems / (t_batch * 1e-3) / 1e9, 4), "unit": UNIT,
         "plain_value": round(total_elems / (t_plain * 1e-3) / 1e9, 4),
         "batched_over_plain": round(t_plain / t_batch, 4),
@@ -457,12 +485,90 @@ def run_batched(args):
         "instances": len(shapes), "waves": len(waves), "total_lde_elements": total_elems,
         "launches_plain": launches_plain, "launches_batched": launches_batch,
         "roots_bit_exact": mismatches == 0, "mismatched_roots": mismatches,
-        "config": {"workload": "64 AIR instances, log2 rows U{16..22}, cols U[16,512], blowup 2 (48) / 4 (16), "
-                               "Poseidon2 W16 arity 4, device budget %.0f GiB per wave" % args.budget_gb},
+        "config": {"workload": shapes_desc + ", Poseidon2 W16 arity 4, device budget %.0f GiB per wave"
+                   % args.budget_gb},
         "n_gpus": 1, "higher_is_better": True, "dtype": "u64", "data": "synthetic (seeded uniform Goldilocks)",
     }
     print(json.dumps(line), flush=True)
     return 0 if mismatches == 0 else 1
+
+
+def run_serving(args):
+    """Served request stream (C5): Poisson arrivals at each rate, request shapes drawn from the C3
+    distribution with a fifth shaped like C4, admitted by the commit server under a device-memory
+    budget; each request's LDE and tree stay resident until it completes and is released.  Reports
+    throughput and p50/p99 request latency (submission to completion) per rate."""
+    import torch
+
+    pkg = load_package()
+    pkg.init(0)
+    lib = pkg.load()
+    rng = np.random.Generator(np.random.PCG64(11))
+    pool = c3_shapes(seed=12, n=args.pool) + [(20, 22, 780)]
+    hosts = []
+    for i, (nb, nbe, nc) in enumerate(pool):
+        h = torch.empty((1 << nb) * nc, dtype=torch.int64, pin_memory=True)
+        lib.b200_fill_random_host(h.data_ptr(), h.numel(), 7000 + i)
+        hosts.append(h)
+    lines = []
+    for rate in [float(r) for r in args.rates.split(",")]:
+        nreq = max(1, min(args.requests, int(rate * args.duration)))
+        picks = [len(pool) - 1 if rng.random() < 0.2 else int(rng.integers(0, len(pool) - 1)) for _ in range(nreq)]
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
+        srv = lib.b200_server_new(0, int(args.serve_budget_gb * 2**30), args.slots)
+        if not srv:
+            raise RuntimeError(lib.b200_last_error().decode())
+        roots = np.zeros((nreq, 4), dtype=np.uint64)
+        ids, lat, done = [None] * nreq, [None] * nreq, 0
+        t0 = time.perf_counter()
+        nxt = 0
+        lat_c = ctypes.c_double()
+        try:
+            while done < nreq:
+                now = time.perf_counter() - t0
+                while nxt < nreq and arrivals[nxt] <= now:
+                    nb, nbe, nc = pool[picks[nxt]]
+                    rid = lib.b200_server_submit(srv, hosts[picks[nxt]].data_ptr(), nb, nbe, nc, 4,
+                                                 roots[nxt].ctypes.data)
+                    if rid < 0:
+                        raise RuntimeError(lib.b200_last_error().decode())
+                    ids[nxt] = rid
+                    nxt += 1
+                for i in range(nxt):
+                    if lat[i] is None:
+                        st = lib.b200_server_status(srv, ids[i], ctypes.byref(lat_c))
+                        if st < 0:
+                            raise RuntimeError(lib.b200_last_error().decode())
+                        if st == 1:
+                            lat[i] = lat_c.value
+                            lib.b200_server_release(srv, ids[i])  # frees its device memory
+                            done += 1
+                if now > args.serve_timeout:
+                    raise RuntimeError("served stream did not finish within %.0f s" % args.serve_timeout)
+                time.sleep(0.001)
+            wall = time.perf_counter() - t0
+        finally:
+            lib.b200_server_free(srv)
+        # same shape, same trace -> same root
+        for k in range(len(pool)):
+            rk = [roots[i] for i in range(nreq) if picks[i] == k]
+            if rk and not all((r == rk[0]).all() for r in rk):
+                raise RuntimeError("served roots differ for one input")
+        elems = sum((1 << pool[p][1]) * pool[p][2] for p in picks)
+        lines.append({"rate_per_s": rate, "requests": nreq, "wall_s": round(wall, 3),
+                      "throughput_gelem_s": round(elems / wall / 1e9, 4),
+                      "p50_ms": round(float(np.percentile(lat, 50)), 2),
+                      "p99_ms": round(float(np.percentile(lat, 99)), 2),
+                      "max_ms": round(float(np.max(lat)), 2)})
+    line = {"metric": "served commit stream: request latency p50/p99 and throughput", "workload": "c5",
+            "unit": "ms", "value": lines[0]["p99_ms"], "higher_is_better": False, "per_rate": lines,
+            "config": {"workload": "Poisson arrivals; shapes: %d drawn from the 64-instance C3 distribution "
+                                   "(80%%) and 2^20 x 780 blowup 4 (20%%); Poseidon2 W16 arity 4" % args.pool,
+                       "device_budget_gib": args.serve_budget_gb, "slots": args.slots,
+                       "requests_per_rate": "min(%d, rate x %.0f s)" % (args.requests, args.duration)},
+            "n_gpus": 1, "dtype": "u64", "data": "synthetic (seeded uniform Goldilocks)"}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def main():
@@ -471,13 +577,23 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c3"], default="c2")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c3", "c3small", "c5"], default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
-    ap.add_argument("--budget-gb", type=float, default=120.0, help="device memory per wave (c3)")
+    ap.add_argument("--budget-gb", type=float, default=120.0, help="device memory per wave (c3, c3small)")
+    ap.add_argument("--no-autotune", action="store_true", help="use the default NTT window plan")
+    ap.add_argument("--rates", default="5,20,80", help="c5: Poisson arrival rates per second")
+    ap.add_argument("--duration", type=float, default=10.0, help="c5: seconds of arrivals per rate")
+    ap.add_argument("--requests", type=int, default=120, help="c5: at most this many requests per rate")
+    ap.add_argument("--pool", type=int, default=6, help="c5: distinct C3-distributed request shapes")
+    ap.add_argument("--slots", type=int, default=4, help="c5: concurrent server slots")
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0, help="c5: server device-memory budget")
+    ap.add_argument("--serve-timeout", type=float, default=300.0, help="c5: give up after this many seconds")
     args = ap.parse_args()
-    if args.workload == "c3":
+    if args.workload in BATCH_SETS:
         return run_batched(args)
+    if args.workload == "c5":
+        return run_serving(args)
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         return run_reference(args, wl)
