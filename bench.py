@@ -538,7 +538,7 @@ def run_serving(args):
                     if lat[i] is None:
                         st = lib.b200_server_status(srv, ids[i], ctypes.byref(lat_c))
                         if st < 0:
-                            raise RuntimeError(lib.b200_last_error().decode())
+                            raise RuntimeError("status %d: %s" % (st, lib.b200_last_error().decode()))
                         if st == 1:
                             lat[i] = lat_c.value
                             lib.b200_server_release(srv, ids[i])  # frees its device memory

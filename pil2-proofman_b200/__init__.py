@@ -53,6 +53,8 @@ _SIGS = {
     "b200_init": (_i32, [_i32]),
     "b200_device_count": (_i32, []),
     "b200_tree_num_elements": (_u64, [_u64, _u64]),
+    "b200_set_native_hash_family": (_i32, [_i32]),
+    "b200_native_hash_family": (_i32, []),
     "b200_lde_scratch_words": (_u64, [_u64, _u64]),
     "b200_lde_device": (_i32, [_vp, _vp, _i32, _u64, _u64, _u64, _vp, _vp]),
     "b200_lde_device_static_scratch": (_i32, [_vp, _vp, _i32, _u64, _u64, _u64, _vp]),
@@ -406,3 +408,13 @@ def pack_rows(trace, col_bits):
             out[:, w + 1] |= v >> np.uint64(64 - o)
         off += nb
     return out
+
+
+# ---------------------------------------------------------------- hash family ----
+def set_native_hash_family(family):
+    """1 = Poseidon1, 2 = Poseidon2 (default) for the native b200_* entry points."""
+    _check(load().b200_set_native_hash_family(family))
+
+
+def native_hash_family():
+    return int(load().b200_native_hash_family())

@@ -1,4 +1,4 @@
-// Poseidon2 row sponge ("linear hash") and arity-k Merkle tree levels.
+// Row sponge ("linear hash") and arity-k Merkle tree levels, Poseidon2 or Poseidon1.
 //
 // Semantics follow the reference CPU path bit for bit:
 //   linear hash  poseidon2_goldilocks.cpp:42-77 — capacity zeroed at the start; every
@@ -15,6 +15,7 @@
 // the same kernel reads the column-major device LDE (rs = 1, cs = nrows; warp loads are
 // 256 B contiguous) or a row-major buffer (rs = ncols, cs = 1).
 #pragma once
+#include "poseidon1.cuh"
 #include "poseidon2.cuh"
 #include "prof.cuh"
 
@@ -22,8 +23,25 @@ namespace merkle {
 
 constexpr int TPB = 128;  // threads per CTA of the hashing kernels (one row / node / state each)
 
+// Hash family (the reference's set_hash_family): 1 = Poseidon1, 2 = Poseidon2.  Both use the same
+// sponge and tree; the Poseidon1 permutation needs a second W x TPB shared area for its matrix
+// steps, right after the state area.
+template <int FAM>
+struct Family {
+    static constexpr int SMEM_AREAS = FAM == 1 ? 2 : 1;
+};
+
+template <int W, int FAM>
+__device__ __forceinline__ void permute_fam(uint64_t *st)
+{
+    if constexpr (FAM == 1)
+        p1::permute_smem<W, TPB>(st, st + W * TPB);
+    else
+        p2::permute_smem<W, TPB>(st);
+}
+
 // Sponge of one row; st = this thread's state slot in a W x TPB shared array.
-template <int W>
+template <int W, int FAM = 2>
 __device__ __forceinline__ void leaf_row(uint64_t *st, uint64_t *__restrict__ digests,
                                          const uint64_t *__restrict__ src, uint64_t rs, uint64_t cs, uint64_t ncols,
                                          uint64_t row)
@@ -45,7 +63,7 @@ __device__ __forceinline__ void leaf_row(uint64_t *st, uint64_t *__restrict__ di
 #pragma unroll
             for (int i = 0; i < RATE; i++) st[i * TPB] = (uint64_t)i < n ? __ldg(p + (done + i) * cs) : 0ull;
         }
-        p2::permute_smem<W, TPB>(st);
+        permute_fam<W, FAM>(st);
     }
     uint64_t *d = digests + row * 4;
     // ncols == 0 leaves the state zeroed: the zero digest
@@ -53,19 +71,19 @@ __device__ __forceinline__ void leaf_row(uint64_t *st, uint64_t *__restrict__ di
     reinterpret_cast<ulonglong2 *>(d)[1] = make_ulonglong2(gl::canon(st[2 * TPB]), gl::canon(st[3 * TPB]));
 }
 
-template <int W>
+template <int W, int FAM = 2>
 __global__ void __launch_bounds__(TPB) leaf_hash_kernel(uint64_t *__restrict__ digests,
                                                         const uint64_t *__restrict__ src, uint64_t rs,
                                                         uint64_t cs, uint64_t ncols, uint64_t nrows)
 {
-    __shared__ uint64_t sm[W * TPB];
+    __shared__ uint64_t sm[Family<FAM>::SMEM_AREAS * W * TPB];
     const uint64_t row = (uint64_t)blockIdx.x * TPB + threadIdx.x;
-    if (row < nrows) leaf_row<W>(sm + threadIdx.x, digests, src, rs, cs, ncols, row);
+    if (row < nrows) leaf_row<W, FAM>(sm + threadIdx.x, digests, src, rs, cs, ncols, row);
 }
 
 // Parent i of one tree level: `pending` child digests at `level`, `pad` zero digests written
 // after them (by the last parent), parents written to `out` (= level + 4*(pending + pad)).
-template <int W>
+template <int W, int FAM = 2>
 __device__ __forceinline__ void node_one(uint64_t *st, uint64_t *__restrict__ level, uint64_t pending, uint64_t pad,
                                          uint64_t parents, uint64_t *__restrict__ out, uint64_t i)
 {
@@ -88,33 +106,33 @@ __device__ __forceinline__ void node_one(uint64_t *st, uint64_t *__restrict__ le
     if (i == parents - 1) {
         for (uint64_t z = 0; z < pad * 4; z++) level[pending * 4 + z] = 0;
     }
-    p2::permute_smem<W, TPB>(st);
+    permute_fam<W, FAM>(st);
     uint64_t *d = out + i * 4;
     reinterpret_cast<ulonglong2 *>(d)[0] = make_ulonglong2(gl::canon(st[0]), gl::canon(st[TPB]));
     reinterpret_cast<ulonglong2 *>(d)[1] = make_ulonglong2(gl::canon(st[2 * TPB]), gl::canon(st[3 * TPB]));
 }
 
-template <int W>
+template <int W, int FAM = 2>
 __global__ void __launch_bounds__(TPB) node_kernel(uint64_t *__restrict__ level, uint64_t pending, uint64_t pad,
                                                    uint64_t parents, uint64_t *__restrict__ out)
 {
-    __shared__ uint64_t sm[W * TPB];
+    __shared__ uint64_t sm[Family<FAM>::SMEM_AREAS * W * TPB];
     const uint64_t i = (uint64_t)blockIdx.x * TPB + threadIdx.x;
-    if (i < parents) node_one<W>(sm + threadIdx.x, level, pending, pad, parents, out, i);
+    if (i < parents) node_one<W, FAM>(sm + threadIdx.x, level, pending, pad, parents, out, i);
 }
 
-// Whole Poseidon2 permutations of n independent states (permute / permuteTrunc checks).
-template <int W>
+// Whole permutations of n independent states (permute / permuteTrunc checks).
+template <int W, int FAM = 2>
 __global__ void __launch_bounds__(TPB) permute_kernel(uint64_t *__restrict__ out, const uint64_t *__restrict__ in,
                                                       uint64_t n)
 {
-    __shared__ uint64_t sm[W * TPB];
+    __shared__ uint64_t sm[Family<FAM>::SMEM_AREAS * W * TPB];
     uint64_t *st = sm + threadIdx.x;
     const uint64_t i = (uint64_t)blockIdx.x * TPB + threadIdx.x;
     if (i >= n) return;
 #pragma unroll
     for (int j = 0; j < W; j++) st[j * TPB] = in[i * W + j];
-    p2::permute_smem<W, TPB>(st);
+    permute_fam<W, FAM>(st);
 #pragma unroll
     for (int j = 0; j < W; j++) out[i * W + j] = gl::canon(st[j * TPB]);
 }
@@ -131,7 +149,7 @@ inline uint64_t tree_num_elements(uint64_t nrows, uint64_t arity)
 }
 
 // Leaf digests and every level up to the root, on `stream`.
-template <int W>
+template <int W, int FAM = 2>
 cudaError_t build_tree(uint64_t *d_tree, const uint64_t *d_src, uint64_t rs, uint64_t cs, uint64_t ncols,
                        uint64_t nrows, cudaStream_t stream)
 {
@@ -140,7 +158,7 @@ cudaError_t build_tree(uint64_t *d_tree, const uint64_t *d_src, uint64_t rs, uin
     const unsigned tpb = TPB;
     {
         prof::Scope ps(prof::LEAF_HASH, stream);
-        leaf_hash_kernel<W><<<(unsigned)((nrows + tpb - 1) / tpb), tpb, 0, stream>>>(d_tree, d_src, rs, cs, ncols,
+        leaf_hash_kernel<W, FAM><<<(unsigned)((nrows + tpb - 1) / tpb), tpb, 0, stream>>>(d_tree, d_src, rs, cs, ncols,
                                                                                        nrows);
         prof::count();
     }
@@ -150,7 +168,7 @@ cudaError_t build_tree(uint64_t *d_tree, const uint64_t *d_src, uint64_t rs, uin
         const uint64_t pad = (ARITY - pending % ARITY) % ARITY;
         const uint64_t parents = (pending + ARITY - 1) / ARITY;
         uint64_t *lvl = d_tree + base;
-        node_kernel<W><<<(unsigned)((parents + tpb - 1) / tpb), tpb, 0, stream>>>(lvl, pending, pad, parents,
+        node_kernel<W, FAM><<<(unsigned)((parents + tpb - 1) / tpb), tpb, 0, stream>>>(lvl, pending, pad, parents,
                                                                                    lvl + (pending + pad) * 4);
         prof::count();
         base += (pending + pad) * 4;
@@ -159,9 +177,18 @@ cudaError_t build_tree(uint64_t *d_tree, const uint64_t *d_src, uint64_t rs, uin
     return cudaGetLastError();
 }
 
+// family: 1 = Poseidon1, otherwise Poseidon2; W = 4 * arity (MerkleTreeGL::merkelize)
 inline cudaError_t build_tree_arity(uint64_t arity, uint64_t *d_tree, const uint64_t *d_src, uint64_t rs,
-                                    uint64_t cs, uint64_t ncols, uint64_t nrows, cudaStream_t stream)
+                                    uint64_t cs, uint64_t ncols, uint64_t nrows, cudaStream_t stream, int family = 2)
 {
+    if (family == 1) {
+        switch (arity) {
+        case 2: return build_tree<8, 1>(d_tree, d_src, rs, cs, ncols, nrows, stream);
+        case 3: return build_tree<12, 1>(d_tree, d_src, rs, cs, ncols, nrows, stream);
+        case 4: return build_tree<16, 1>(d_tree, d_src, rs, cs, ncols, nrows, stream);
+        default: return cudaErrorInvalidValue;
+        }
+    }
     switch (arity) {
     case 2: return build_tree<8>(d_tree, d_src, rs, cs, ncols, nrows, stream);
     case 3: return build_tree<12>(d_tree, d_src, rs, cs, ncols, nrows, stream);

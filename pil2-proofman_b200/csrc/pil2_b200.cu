@@ -90,6 +90,20 @@ static int check_shape(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64
     return B200_OK;
 }
 
+// Hash family of the native b200_* entry points (1 = Poseidon1, 2 = Poseidon2, the default).
+// The reference entry points follow set_hash_family instead, which the reference allows to be
+// set once per process.
+static std::atomic<int> g_native_family{2};
+
+extern "C" int b200_set_native_hash_family(int family)
+{
+    if (family != 1 && family != 2) return set_err(B200_EINVAL, "hash family must be 1 (Poseidon1) or 2 (Poseidon2)");
+    g_native_family.store(family);
+    return B200_OK;
+}
+
+extern "C" int b200_native_hash_family(void) { return g_native_family.load(); }
+
 // ------------------------------------------------------- device-pointer API ----
 extern "C" int b200_lde_device(uint64_t *d_lde, const uint64_t *d_trace, int trace_rowmajor, uint64_t nBits,
                                uint64_t nBitsExt, uint64_t nCols, uint64_t *d_scratch, void *stream)
@@ -154,13 +168,15 @@ extern "C" int b200_merkletree_device(uint64_t *d_tree, const uint64_t *d_src, u
     int rc = ensure_init_current();
     if (rc) return rc;
     if (nRows && (!d_tree || (nCols && !d_src))) return set_err(B200_EINVAL, "null buffer");
-    CK(merkle::build_tree_arity(arity, d_tree, d_src, rs, cs, nCols, nRows, (cudaStream_t)stream), "merkletree");
+    CK(merkle::build_tree_arity(arity, d_tree, d_src, rs, cs, nCols, nRows, (cudaStream_t)stream,
+                                g_native_family.load()),
+       "merkletree");
     return B200_OK;
 }
 
-extern "C" int b200_commit_device(uint64_t *root_host, uint64_t *d_lde, uint64_t *d_tree, const uint64_t *d_trace,
-                                  int trace_rowmajor, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols,
-                                  uint64_t arity, uint64_t *d_scratch, void *stream)
+static int commit_device_fam(uint64_t *root_host, uint64_t *d_lde, uint64_t *d_tree, const uint64_t *d_trace,
+                             int trace_rowmajor, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t arity,
+                             uint64_t *d_scratch, void *stream, int family)
 {
     int rc = check_shape(nBits, nBitsExt, nCols, arity);
     if (rc) return rc;
@@ -170,13 +186,21 @@ extern "C" int b200_commit_device(uint64_t *root_host, uint64_t *d_lde, uint64_t
     if (!d_tree || (nCols && (!d_lde || !d_trace || !d_scratch))) return set_err(B200_EINVAL, "null buffer");
     CK(ntt::lde(d_lde, d_trace, trace_rowmajor != 0, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, d_scratch, s),
        "lde");
-    CK(merkle::build_tree_arity(arity, d_tree, d_lde, 1, NExt, nCols, NExt, s), "merkletree");
+    CK(merkle::build_tree_arity(arity, d_tree, d_lde, 1, NExt, nCols, NExt, s, family), "merkletree");
     if (root_host) {
         const uint64_t total = merkle::tree_num_elements(NExt, arity);
         CK(cudaMemcpyAsync(root_host, d_tree + total - 4, 32, cudaMemcpyDeviceToHost, s), "root D2H");
         CK(cudaStreamSynchronize(s), "sync");
     }
     return B200_OK;
+}
+
+extern "C" int b200_commit_device(uint64_t *root_host, uint64_t *d_lde, uint64_t *d_tree, const uint64_t *d_trace,
+                                  int trace_rowmajor, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols,
+                                  uint64_t arity, uint64_t *d_scratch, void *stream)
+{
+    return commit_device_fam(root_host, d_lde, d_tree, d_trace, trace_rowmajor, nBits, nBitsExt, nCols, arity,
+                             d_scratch, stream, g_native_family.load());
 }
 
 extern "C" int b200_permute_device(uint64_t *d_out, const uint64_t *d_in, uint64_t n, uint64_t width, void *stream)
@@ -186,10 +210,20 @@ extern "C" int b200_permute_device(uint64_t *d_out, const uint64_t *d_in, uint64
     if (n == 0) return B200_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const unsigned tpb = 128, blocks = (unsigned)((n + tpb - 1) / tpb);
+    const bool p1 = g_native_family.load() == 1;
     switch (width) {
-    case 8: merkle::permute_kernel<8><<<blocks, tpb, 0, s>>>(d_out, d_in, n); break;
-    case 12: merkle::permute_kernel<12><<<blocks, tpb, 0, s>>>(d_out, d_in, n); break;
-    case 16: merkle::permute_kernel<16><<<blocks, tpb, 0, s>>>(d_out, d_in, n); break;
+    case 8:
+        if (p1) merkle::permute_kernel<8, 1><<<blocks, tpb, 0, s>>>(d_out, d_in, n);
+        else merkle::permute_kernel<8><<<blocks, tpb, 0, s>>>(d_out, d_in, n);
+        break;
+    case 12:
+        if (p1) merkle::permute_kernel<12, 1><<<blocks, tpb, 0, s>>>(d_out, d_in, n);
+        else merkle::permute_kernel<12><<<blocks, tpb, 0, s>>>(d_out, d_in, n);
+        break;
+    case 16:
+        if (p1) merkle::permute_kernel<16, 1><<<blocks, tpb, 0, s>>>(d_out, d_in, n);
+        else merkle::permute_kernel<16><<<blocks, tpb, 0, s>>>(d_out, d_in, n);
+        break;
     default: return set_err(B200_EINVAL, "width must be 8, 12 or 16");
     }
     CK(cudaGetLastError(), "permute");
@@ -299,9 +333,9 @@ extern "C" void set_hash_family(uint8_t fam)
 static int check_family()
 {
     int f = g_hash_family.load();
-    if (f == 2) return B200_OK;
-    if (f == 0) return set_err(B200_EFAMILY, "hash family not set: call set_hash_family(2) first");
-    return set_err(B200_EFAMILY, "only the Poseidon2 family (2) is provided by this library");
+    if (f == 1 || f == 2) return B200_OK;
+    if (f == 0) return set_err(B200_EFAMILY, "hash family not set: call set_hash_family(1 or 2) first");
+    return set_err(B200_EFAMILY, "unknown hash family (1 = Poseidon1, 2 = Poseidon2)");
 }
 
 extern "C" void init_gpu_setup(uint64_t arity)
@@ -457,7 +491,8 @@ static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_
     CK(cudaEventRecord(s.h2d_done, s.stream), "event");
     CK(ntt::lde(s.d_lde, s.d_trace, true, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, s.d_scratch, s.stream),
        "lde");
-    CK(merkle::build_tree_arity(arity, s.d_tree, s.d_lde, 1, NExt, nCols, NExt, s.stream), "merkletree");
+    CK(merkle::build_tree_arity(arity, s.d_tree, s.d_lde, 1, NExt, nCols, NExt, s.stream, g_hash_family.load()),
+       "merkletree");
     CK(cudaMemcpyAsync(s.h_root, s.d_tree + tsz - 4, 32, cudaMemcpyDeviceToHost, s.stream), "root D2H");
     CK(cudaEventRecord(s.end, s.stream), "event");
     (void)b;
@@ -636,8 +671,8 @@ extern "C" void calculate_const_tree(void *pStarkInfo, void *pConstPolsAddress, 
     cudaStream_t s;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return;
     if (N * nCols) cudaMemcpyAsync(tr.p, pConstPolsAddress, N * nCols * 8, cudaMemcpyHostToDevice, s);
-    if (b200_commit_device(nullptr, d_tree, d_tree + NExt * nCols, tr.p, 1, sh->nBits, sh->nBitsExt, nCols,
-                           sh->arity, sc.p, s) == B200_OK)
+    if (commit_device_fam(nullptr, d_tree, d_tree + NExt * nCols, tr.p, 1, sh->nBits, sh->nBitsExt, nCols,
+                           sh->arity, sc.p, s, g_hash_family.load()) == B200_OK)
         cudaMemcpyAsync(pConstTree, d_tree, total * 8, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
     cudaStreamDestroy(s);
@@ -752,7 +787,7 @@ extern "C" int b200_commit_q_device(uint64_t *root_host, uint64_t *d_cmq, uint64
     CK(ntt::lde_q(d_cmq, d_q, q_rowmajor != 0, (uint32_t)nBits, (uint32_t)nBitsExt, (uint32_t)qDeg, (uint32_t)qDim,
                   d_scratch, s),
        "Q extension");
-    CK(merkle::build_tree_arity(arity, d_tree, d_cmq, 1, NExt, ncols, NExt, s), "merkletree");
+    CK(merkle::build_tree_arity(arity, d_tree, d_cmq, 1, NExt, ncols, NExt, s, g_native_family.load()), "merkletree");
     if (root_host) {
         const uint64_t total = merkle::tree_num_elements(NExt, arity);
         CK(cudaMemcpyAsync(root_host, d_tree + total - 4, 32, cudaMemcpyDeviceToHost, s), "root D2H");
@@ -910,7 +945,7 @@ extern "C" int b200_commit_packed_device(uint64_t *root_host, uint64_t *d_lde, u
         // the trace now sits column-major in the scratch; the LDE transforms it in place
         CK(ntt::lde(d_lde, d_scratch, false, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, d_scratch, s), "lde");
     }
-    CK(merkle::build_tree_arity(arity, d_tree, d_lde, 1, NExt, nCols, NExt, s), "merkletree");
+    CK(merkle::build_tree_arity(arity, d_tree, d_lde, 1, NExt, nCols, NExt, s, g_native_family.load()), "merkletree");
     if (root_host) {
         const uint64_t total = merkle::tree_num_elements(NExt, arity);
         CK(cudaMemcpyAsync(root_host, d_tree + total - 4, 32, cudaMemcpyDeviceToHost, s), "root D2H");

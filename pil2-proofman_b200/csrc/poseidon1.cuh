@@ -1,0 +1,194 @@
+// Poseidon1 over Goldilocks (hash family 1), widths 8 / 12 / 16.
+//
+// The reference's optimised round structure (poseidon_goldilocks.cpp:13-51): add C_0; three
+// full rounds (x^7, add the next round's constants, state <- M^T x); x^7, add C_4, state <- P^T x;
+// 22 sparse partial rounds (x0 <- x0^7 + c_r; x0' = <x, S_r[0..W)>; x_i += x0 * S_r[W-1+i] for
+// i >= 1); three full rounds with M; x^7 and M.  mvp_ (poseidon_goldilocks.hpp:210-224) applies
+// its matrix transposed: out_i = sum_j mat[j][i] * x_j.
+//
+// Arithmetic:
+//   * M has entries below 2^7, so each output of M^T x is accumulated as two 64-bit sums of
+//     32x32 products (low and high halves of x_j), combined into a 96-bit value and folded once.
+//   * P and the partial-round vectors S are full field elements: the dot products accumulate
+//     128-bit products in 160 bits and reduce once (2^128 = -2^32 mod p).
+// State in shared memory, word i of this thread at st[i*TPB], like the Poseidon2 kernels; the
+// matrix steps write to a second W x TPB area and copy back.
+#pragma once
+#include "gl64.cuh"
+#include "poseidon1_constants.h"
+
+__constant__ uint64_t c_p1_C8[P1_NC_8] = {P1_C8_LIST};
+__constant__ uint64_t c_p1_M8[64] = {P1_M8_LIST};
+__constant__ uint64_t c_p1_P8[64] = {P1_P8_LIST};
+__constant__ uint64_t c_p1_S8[P1_NS_8] = {P1_S8_LIST};
+__constant__ uint64_t c_p1_C12[P1_NC_12] = {P1_C12_LIST};
+__constant__ uint64_t c_p1_M12[144] = {P1_M12_LIST};
+__constant__ uint64_t c_p1_P12[144] = {P1_P12_LIST};
+__constant__ uint64_t c_p1_S12[P1_NS_12] = {P1_S12_LIST};
+__constant__ uint64_t c_p1_C16[P1_NC_16] = {P1_C16_LIST};
+__constant__ uint64_t c_p1_M16[256] = {P1_M16_LIST};
+__constant__ uint64_t c_p1_P16[256] = {P1_P16_LIST};
+__constant__ uint64_t c_p1_S16[P1_NS_16] = {P1_S16_LIST};
+
+namespace p1 {
+
+template <int W> struct Tab;
+template <> struct Tab<8> {
+    static __device__ __forceinline__ const uint64_t *C() { return c_p1_C8; }
+    static __device__ __forceinline__ const uint64_t *M() { return c_p1_M8; }
+    static __device__ __forceinline__ const uint64_t *P() { return c_p1_P8; }
+    static __device__ __forceinline__ const uint64_t *S() { return c_p1_S8; }
+};
+template <> struct Tab<12> {
+    static __device__ __forceinline__ const uint64_t *C() { return c_p1_C12; }
+    static __device__ __forceinline__ const uint64_t *M() { return c_p1_M12; }
+    static __device__ __forceinline__ const uint64_t *P() { return c_p1_P12; }
+    static __device__ __forceinline__ const uint64_t *S() { return c_p1_S12; }
+};
+template <> struct Tab<16> {
+    static __device__ __forceinline__ const uint64_t *C() { return c_p1_C16; }
+    static __device__ __forceinline__ const uint64_t *M() { return c_p1_M16; }
+    static __device__ __forceinline__ const uint64_t *P() { return c_p1_P16; }
+    static __device__ __forceinline__ const uint64_t *S() { return c_p1_S16; }
+};
+
+constexpr int NPARTIAL = P1_NPARTIAL;
+
+// 160-bit accumulator of 128-bit products
+struct Acc160 {
+    uint32_t w[5];
+};
+
+__device__ __forceinline__ void acc160_mul_add(Acc160 &a, uint64_t x, uint64_t y)
+{
+    uint32_t r0, r1, r2, r3;
+    gl::mul128(x, y, r0, r1, r2, r3);
+    asm("add.cc.u32  %0, %0, %5;\n\t"
+        "addc.cc.u32 %1, %1, %6;\n\t"
+        "addc.cc.u32 %2, %2, %7;\n\t"
+        "addc.cc.u32 %3, %3, %8;\n\t"
+        "addc.u32    %4, %4, 0;\n\t"
+        : "+r"(a.w[0]), "+r"(a.w[1]), "+r"(a.w[2]), "+r"(a.w[3]), "+r"(a.w[4])
+        : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
+}
+
+// x = A + w4 * 2^128 with 2^128 = -2^32 (mod p): reduce A, then subtract w4 * 2^32 (< p)
+__device__ __forceinline__ uint64_t acc160_reduce(const Acc160 &a)
+{
+    const uint64_t y = gl::reduce128(a.w[0], a.w[1], a.w[2], a.w[3]);
+    return gl::sub(y, (uint64_t)a.w[4] << 32);
+}
+
+// out_i = sum_j M[j][i] x_j for the small-entry MDS matrix (entries < 2^32)
+template <int W, int TPB>
+__device__ __forceinline__ void mvp_small(uint64_t *st, uint64_t *tmp)
+{
+    const uint64_t *M = Tab<W>::M();
+#pragma unroll 1
+    for (int i0 = 0; i0 < W; i0 += 4) {
+        uint64_t L[4] = {0, 0, 0, 0}, H[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < W; j++) {
+            const uint64_t x = st[j * TPB];
+            const uint32_t xl = gl::lo32(x), xh = gl::hi32(x);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint32_t m = (uint32_t)M[j * W + i0 + u];
+                asm("mad.wide.u32 %0, %1, %2, %0;" : "+l"(L[u]) : "r"(xl), "r"(m));
+                asm("mad.wide.u32 %0, %1, %2, %0;" : "+l"(H[u]) : "r"(xh), "r"(m));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            // L + H * 2^32 as three words (L, H < 2^44: no overflow)
+            gl::Acc a;
+            uint32_t c;
+            a.w0 = gl::lo32(L[u]);
+            asm("add.cc.u32 %0, %2, %3;\n\t"
+                "addc.u32   %1, 0, 0;\n\t"
+                : "=r"(a.w1), "=r"(c)
+                : "r"(gl::hi32(L[u])), "r"(gl::lo32(H[u])));
+            a.w2 = gl::hi32(H[u]) + c;
+            tmp[(i0 + u) * TPB] = gl::acc_reduce(a);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < W; i++) st[i * TPB] = tmp[i * TPB];
+}
+
+// out_i = sum_j P[j][i] x_j for a matrix of full field elements
+template <int W, int TPB>
+__device__ __forceinline__ void mvp_full(uint64_t *st, uint64_t *tmp, const uint64_t *P)
+{
+#pragma unroll 1
+    for (int i0 = 0; i0 < W; i0 += 2) {
+        Acc160 a0 = {{0, 0, 0, 0, 0}}, a1 = {{0, 0, 0, 0, 0}};
+#pragma unroll 4
+        for (int j = 0; j < W; j++) {
+            const uint64_t x = st[j * TPB];
+            acc160_mul_add(a0, x, P[j * W + i0]);
+            acc160_mul_add(a1, x, P[j * W + i0 + 1]);
+        }
+        tmp[i0 * TPB] = acc160_reduce(a0);
+        tmp[(i0 + 1) * TPB] = acc160_reduce(a1);
+    }
+#pragma unroll
+    for (int i = 0; i < W; i++) st[i * TPB] = tmp[i * TPB];
+}
+
+// x^7 then + c (c canonical) on every word
+template <int W, int TPB>
+__device__ __forceinline__ void sbox_add(uint64_t *st, const uint64_t *c)
+{
+#pragma unroll 1
+    for (int q = 0; q < W; q += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const uint64_t x = gl::pow7(st[(q + u) * TPB]);
+            st[(q + u) * TPB] = c ? gl::add_c(x, c[q + u]) : x;
+        }
+    }
+}
+
+// The permutation of the thread's state st[i*TPB] (loose words in, loose words out);
+// tmp: a second W x TPB area of the thread.
+template <int W, int TPB>
+__device__ __forceinline__ void permute_smem(uint64_t *st, uint64_t *tmp)
+{
+    const uint64_t *C = Tab<W>::C();
+    const uint64_t *S = Tab<W>::S();
+#pragma unroll
+    for (int i = 0; i < W; i++) st[i * TPB] = gl::add_c(st[i * TPB], C[i]);
+#pragma unroll 1
+    for (int r = 0; r < 3; r++) {
+        sbox_add<W, TPB>(st, C + (r + 1) * W);
+        mvp_small<W, TPB>(st, tmp);
+    }
+    sbox_add<W, TPB>(st, C + 4 * W);
+    mvp_full<W, TPB>(st, tmp, Tab<W>::P());
+    uint64_t x0 = st[0];
+#pragma unroll 1
+    for (int r = 0; r < NPARTIAL; r++) {
+        const uint64_t *Sr = S + (2 * W - 1) * r;
+        x0 = gl::add_c(gl::pow7(x0), C[5 * W + r]);
+        Acc160 a = {{0, 0, 0, 0, 0}};
+        acc160_mul_add(a, x0, Sr[0]);
+#pragma unroll 4
+        for (int i = 1; i < W; i++) {
+            const uint64_t xi = st[i * TPB];
+            acc160_mul_add(a, xi, Sr[i]);
+            st[i * TPB] = gl::mul_add(x0, Sr[W - 1 + i], xi);
+        }
+        x0 = acc160_reduce(a);
+    }
+    st[0] = x0;
+#pragma unroll 1
+    for (int r = 0; r < 3; r++) {
+        sbox_add<W, TPB>(st, C + 5 * W + NPARTIAL + r * W);
+        mvp_small<W, TPB>(st, tmp);
+    }
+    sbox_add<W, TPB>(st, nullptr);
+    mvp_small<W, TPB>(st, tmp);
+}
+
+}  // namespace p1

@@ -35,6 +35,7 @@ struct Request {
     int status = 0;  // 0 queued, 1 running, 2 done, < 0 error
     bool released = false;
     double t_submit = 0, t_admit = 0, t_done = 0;
+    std::string err;  // reason of a failed request (reported to the caller by status())
     uint64_t bytes() const { return 8 * (2 * words_trace + words_lde + words_tree); }
 };
 
@@ -134,6 +135,19 @@ class Server {
         return r->id;
     }
 
+    // all four device buffers of a request, or none
+    bool alloc_request(Request *r, cudaStream_t s)
+    {
+        if (cudaMallocAsync((void **)&r->d_trace, 8 * (r->words_trace ? r->words_trace : 1), s) == cudaSuccess &&
+            cudaMallocAsync((void **)&r->d_scratch, 8 * (r->words_trace ? r->words_trace : 1), s) == cudaSuccess &&
+            cudaMallocAsync((void **)&r->d_lde, 8 * (r->words_lde ? r->words_lde : 1), s) == cudaSuccess &&
+            cudaMallocAsync((void **)&r->d_tree, 8 * r->words_tree, s) == cudaSuccess)
+            return true;
+        cudaGetLastError();
+        free_buffers(r, s);
+        return false;
+    }
+
     // admit the head of the queue onto a free slot; caller holds mu
     bool admit_one()
     {
@@ -154,16 +168,22 @@ class Server {
         if (!r->h_root && cudaMallocHost((void **)&r->h_root, 32) != cudaSuccess) rc = B200_ENOMEM;
         if (!rc && !r->done && cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming) != cudaSuccess)
             rc = B200_ECUDA;
-        if (!rc && (cudaMallocAsync((void **)&r->d_trace, 8 * (r->words_trace ? r->words_trace : 1), s) ||
-                    cudaMallocAsync((void **)&r->d_scratch, 8 * (r->words_trace ? r->words_trace : 1), s) ||
-                    cudaMallocAsync((void **)&r->d_lde, 8 * (r->words_lde ? r->words_lde : 1), s) ||
-                    cudaMallocAsync((void **)&r->d_tree, 8 * r->words_tree, s)))
-            rc = B200_ENOMEM;
+        if (!rc && !alloc_request(r, s)) {
+            // The pool keeps freed blocks cached; when the cached sizes do not fit this request,
+            // return them to the device (after the running requests' frees have executed) and retry.
+            for (cudaStream_t t : streams) cudaStreamSynchronize(t);
+            cudaMemPoolTrimTo(pool, 0);
+            cudaGetLastError();
+            if (!alloc_request(r, s)) {
+                rc = B200_ENOMEM;
+                r->err = "device buffers for the request could not be allocated";
+            }
+        }
         if (!rc && r->words_trace &&
             cudaMemcpyAsync(r->d_trace, r->trace, 8 * r->words_trace, cudaMemcpyHostToDevice, s) != cudaSuccess)
             rc = B200_ECUDA;
-        if (!rc) rc = b200_commit_device(nullptr, r->d_lde, r->d_tree, r->d_trace, 1, r->nBits, r->nBitsExt, r->nCols,
-                                         r->arity, r->d_scratch, s);
+        if (!rc) rc = commit_device_fam(nullptr, r->d_lde, r->d_tree, r->d_trace, 1, r->nBits, r->nBitsExt, r->nCols,
+                                        r->arity, r->d_scratch, s, 2);
         if (!rc && cudaMemcpyAsync(r->h_root, r->d_tree + r->words_tree - 4, 32, cudaMemcpyDeviceToHost, s) !=
                        cudaSuccess)
             rc = B200_ECUDA;
@@ -176,6 +196,7 @@ class Server {
         }
         if (rc) {
             free_buffers(r, s);
+            if (r->err.empty()) r->err = "request failed on the device (CUDA error)";
             r->status = rc;
             r->t_done = now_ms();
             return true;
@@ -227,7 +248,8 @@ class Server {
         Request *r = it->second;
         if (r->status == 2 || r->status < 0) {
             if (latency_ms) *latency_ms = r->t_done - r->t_submit;
-            return r->status == 2 ? 1 : r->status;
+            if (r->status < 0) return set_err(r->status, "request " + std::to_string(id) + ": " + r->err);
+            return 1;
         }
         return 0;
     }
@@ -267,6 +289,10 @@ extern "C" void *b200_server_new(int device, uint64_t budget_bytes, uint32_t slo
 {
     if (slots == 0 || slots > 64) {
         set_err(B200_EINVAL, "slots must be 1..64");
+        return nullptr;
+    }
+    if (g_native_family.load() != 2) {
+        set_err(B200_EFAMILY, "the commit server hashes with Poseidon2 only");
         return nullptr;
     }
     auto *s = new serve::Server();
