@@ -47,6 +47,10 @@ WORKLOADS = {
 METRIC = "LDE+Merkle commit GElem/s (NExt x nCols per second), bit-exact roots"
 UNIT = "GElem/s"
 P2_MULS = {8: 8 * 8 * 4 + 22 * (4 + 8), 12: 8 * 12 * 4 + 22 * (4 + 12), 16: 8 * 16 * 4 + 22 * (4 + 16)}
+# Poseidon1: x^7 on every word of 8 full rounds, the dense pre-partial matrix P (W^2), and per partial
+# round x0^7, a W-term dot product and W-1 products; the small-entry MDS M adds 32x64 products only
+P1_MULS = {w: 8 * w * 4 + w * w + 22 * (4 + w + w - 1) for w in (8, 12, 16)}
+HASH_NAME = {1: "Poseidon1", 2: "Poseidon2"}
 IMAD_PER_MUL = 8  # four 32x32->64 partial products, two IMAD-pipe ops each
 
 
@@ -150,13 +154,13 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def time_reference_cpu(wl, reps, warmup):
+def time_reference_cpu(wl, reps, warmup, family=2):
     """Reference CPU LDE + tree on a row sample; returns (GElem/s, seconds per rep, threads, sample)."""
     sys.path.insert(0, REPO)
     import oracle  # CPU baseline leg only
 
     threads = cpu_threads()
-    ref = oracle.RefCPU(threads=threads)
+    ref = oracle.RefCPU(threads=threads, family=family)
     nb = wl["sample_nbits"]
     b = wl["nbits_ext"] - wl["nbits"]
     ncols, arity = wl["ncols"], wl["arity"]
@@ -174,8 +178,9 @@ def time_reference_cpu(wl, reps, warmup):
             times.append(t1 - t0)
     sec = statistics.median(times)
     elems = (1 << (nb + b)) * ncols
-    sample = "%d x %d trace -> %d x %d LDE + W%d arity-%d tree (1/%d of the rows), %s build" % (
-        1 << nb, ncols, 1 << (nb + b), ncols, 4 * arity, arity, 1 << (wl["nbits"] - nb), ref.variant)
+    sample = "%d x %d trace -> %d x %d LDE + %s W%d arity-%d tree (1/%d of the rows), %s build" % (
+        1 << nb, ncols, 1 << (nb + b), ncols, HASH_NAME[family], 4 * arity, arity, 1 << (wl["nbits"] - nb),
+        ref.variant)
     return elems / sec / 1e9, sec, threads, sample
 
 
@@ -183,7 +188,7 @@ def run_reference(args, wl):
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    val, sec, threads, sample = time_reference_cpu(wl, args.steps, args.warmup)
+    val, sec, threads, sample = time_reference_cpu(wl, args.steps, args.warmup, args.hash_family)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(val, 6), "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3),
@@ -211,6 +216,7 @@ def run_ours(args, wl):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     pkg = load_package()
     pkg.init(local)
+    pkg.set_native_hash_family(args.hash_family)
     nbits, nbe, ncols, arity = wl["nbits"], wl["nbits_ext"], wl["ncols"], wl["arity"]
     N, NExt = 1 << nbits, 1 << nbe
     elems = NExt * ncols
@@ -270,20 +276,21 @@ def run_ours(args, wl):
     w = 4 * arity
     perms_per_row = max(1, -(-ncols // (w - 4)))
     leaf_ms = cats["leaf_hash"][0] / max(1, cats["leaf_hash"][1])
-    muls = NExt * perms_per_row * P2_MULS[w]
+    mul_table = P1_MULS if args.hash_family == 1 else P2_MULS
+    muls = NExt * perms_per_row * mul_table[w]
     achieved_gmul = muls / (leaf_ms * 1e-3) / 1e9
     peak_gmul = imad / IMAD_PER_MUL
     ntt_ms = sum(cats[c][0] for c in ("transpose", "ntt_inverse", "ntt_forward")) / args.steps
     ntt_bytes = 8 * ncols * (N + NExt)
     ntt_gbs = ntt_bytes / (ntt_ms * 1e-3) / 1e9
     roofline = {
-        "kernel": "leaf_hash_kernel<16>",
+        "kernel": "leaf_hash_kernel<%d,%d>" % (w, args.hash_family),
         "bound": "int32_imad",
         "achieved": round(achieved_gmul, 2), "peak": round(peak_gmul, 2), "unit": "G Goldilocks-mul/s",
         "frac": round(achieved_gmul / peak_gmul, 4),
-        "traffic": ncu_traffic("leaf_hash_kernel", args.workload),
+        "traffic": ncu_traffic("leaf_hash_kernel", args.workload) if args.hash_family == 2 else None,
         "algorithmic": "%d permutations/row x %d muls (W%d) per row, %d IMAD-pipe ops per mul; peak = "
-                       "measured IMAD probe %.0f G/s / %d" % (perms_per_row, P2_MULS[w], w, IMAD_PER_MUL, imad,
+                       "measured IMAD probe %.0f G/s / %d" % (perms_per_row, mul_table[w], w, IMAD_PER_MUL, imad,
                                                              IMAD_PER_MUL),
         "ntt": {"bound": "hbm", "achieved": round(ntt_gbs, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                 "frac": round(ntt_gbs / peaks.get("hbm_gbs", 6650.0), 4),
@@ -303,7 +310,7 @@ def run_ours(args, wl):
     del trace, scratch, lde, tree
     torch.cuda.empty_cache()
     lib = pkg.load()
-    pkg.set_hash_family(2)
+    pkg.set_hash_family(args.hash_family)
     bufs = pkg.DeviceBuffers(arity=arity, n_streams=2)
     shape = pkg.StarkShape(nbits, nbe, ncols, arity)
     params = pkg.StepsParams()
@@ -343,7 +350,7 @@ def finish(args, wl, pkg, dist, rank, world, value, ms, launches, kernel_ms, roo
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform Goldilocks)",
         "config": {"workload": wl["desc"], "nBits": nbits, "nBitsExt": nbe, "nCols": ncols, "arity": arity,
-                   "hash": "Poseidon2 W%d" % w, "parallelism": "instance per GPU" if world > 1 else "single GPU",
+                   "hash": "%s W%d" % (HASH_NAME[args.hash_family], w), "parallelism": "instance per GPU" if world > 1 else "single GPU",
                    "l2": "inputs (%.1f GB) larger than L2; no flush" % (N * ncols * 8 / 1e9)},
         "e2e": e2e_obj,
         "gpu_launches": int(launches),
@@ -354,7 +361,7 @@ def finish(args, wl, pkg, dist, rank, world, value, ms, launches, kernel_ms, roo
         "root": [hex(int(v)) for v in roots[0]] if rank == 0 else None,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        val, sec, threads, sample = time_reference_cpu(wl, 1, 0)
+        val, sec, threads, sample = time_reference_cpu(wl, 1, 0, args.hash_family)
         line["cpu_baseline"] = {"value": round(val, 6), "unit": UNIT, "cores": threads, "kind": "reference",
                                 "sample": sample}
     if dist is not None:
@@ -582,6 +589,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--budget-gb", type=float, default=120.0, help="device memory per wave (c3, c3small)")
     ap.add_argument("--no-autotune", action="store_true", help="use the default NTT window plan")
+    ap.add_argument("--hash-family", type=int, choices=[1, 2], default=2,
+                    help="1 = Poseidon1, 2 = Poseidon2 (single-instance workloads)")
     ap.add_argument("--rates", default="5,20,80", help="c5: Poisson arrival rates per second")
     ap.add_argument("--duration", type=float, default=10.0, help="c5: seconds of arrivals per rate")
     ap.add_argument("--requests", type=int, default=120, help="c5: at most this many requests per rate")
