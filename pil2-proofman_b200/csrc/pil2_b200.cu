@@ -798,15 +798,17 @@ extern "C" int b200_commit_q_device(uint64_t *root_host, uint64_t *d_cmq, uint64
 
 // ------------------------------------------------------------ plan autotuner ----
 // Times lde() under each candidate plan (largest first window kf, largest later window kr,
-// both in 8..12) on a probe of min(nCols, 64) columns of seeded data, and keeps the fastest for
-// the shape's column bucket.  Untimed set-up for callers; every plan computes the same values.
+// both in 8..12) on a probe of min(nCols, 256) columns of seeded data, interleaving each
+// candidate's runs with the default plan's, and keeps a candidate only if it beats the default by
+// more than 3 % (probe timings of plans that differ by less are noise, and a narrower probe can
+// rank plans differently from the full width).  Untimed set-up; every plan computes the same values.
 extern "C" int b200_autotune_lde(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, double *best_ms,
                                  uint32_t *kfirst, uint32_t *krest)
 {
     int rc = check_shape(nBits, nBitsExt, nCols, 4);
     if (rc) return rc;
     if ((rc = ensure_init_current())) return rc;
-    const uint64_t probe = nCols < 64 ? (nCols ? nCols : 1) : 64;
+    const uint64_t probe = nCols < 256 ? (nCols ? nCols : 1) : 256;
     const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
     uint64_t *d_trace = nullptr, *d_lde = nullptr, *d_scr = nullptr;
     cudaStream_t s = nullptr;
@@ -827,33 +829,58 @@ extern "C" int b200_autotune_lde(uint64_t nBits, uint64_t nBitsExt, uint64_t nCo
         return set_err(B200_ENOMEM, "autotune buffers");
     }
     synth::fill_kernel<<<(unsigned)((N * probe + 255) / 256), 256, 0, s>>>(d_trace, N * probe, 99);
-    double best = 1e30;
-    ntt::Tune bt{};
+    // best of three runs of plan t (after one warm-up); < 0 on a CUDA error
+    auto time_plan = [&](ntt::Tune t) -> double {
+        ntt::set_tuned((uint32_t)nBits, (uint32_t)nBitsExt, nCols, t);
+        float best_ms_t = 1e30f;
+        for (int it = 0; it < 4; it++) {
+            cudaEventRecord(e0, s);
+            if (ntt::lde(d_lde, d_trace, true, (uint32_t)nBits, (uint32_t)nBitsExt, probe, d_scr, s) != cudaSuccess)
+                return -1;
+            cudaEventRecord(e1, s);
+            float ms = 0;
+            if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+                return -1;
+            if (it > 0 && ms < best_ms_t) best_ms_t = ms;
+        }
+        return best_ms_t;
+    };
+    const ntt::Tune def{};
+    ntt::Tune bt = def;
+    double best = 1e30, best_ratio = 1.0;
+    // the windows a plan produces (candidates with the default's windows need no run)
+    auto windows = [&](ntt::Tune t) {
+        std::vector<uint32_t> v;
+        ntt::Window w[8];
+        int n1 = nBits ? ntt::plan_windows(0, (uint32_t)nBits, w, 8, t.kfirst, t.krest) : 0;
+        for (int i = 0; i < n1; i++) v.insert(v.end(), {w[i].s0, w[i].k, w[i].lgL});
+        v.push_back(99);
+        int n2 = ntt::plan_windows((uint32_t)(nBitsExt - nBits), (uint32_t)nBitsExt, w, 8, t.kfirst, t.krest);
+        for (int i = 0; i < n2; i++) v.insert(v.end(), {w[i].s0, w[i].k, w[i].lgL});
+        if (n1 < 0 || n2 < 0) v.clear();
+        return v;
+    };
+    const std::vector<uint32_t> wdef = windows(def);
     for (uint32_t kf = 8; kf <= NTT_KMAX; kf++) {
         for (uint32_t kr = 8; kr <= NTT_KMAX; kr++) {
-            ntt::set_tuned((uint32_t)nBits, (uint32_t)nBitsExt, nCols, ntt::Tune{kf, kr});
-            // one warm-up, then the best of three
-            float ms_best = 1e30f;
-            bool ok = true;
-            for (int it = 0; it < 4 && ok; it++) {
-                cudaEventRecord(e0, s);
-                ok = ntt::lde(d_lde, d_trace, true, (uint32_t)nBits, (uint32_t)nBitsExt, probe, d_scr, s) ==
-                     cudaSuccess;
-                cudaEventRecord(e1, s);
-                float ms = 0;
-                if (ok) ok = cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
-                if (it > 0 && ms < ms_best) ms_best = ms;
-            }
-            if (!ok) {
+            const std::vector<uint32_t> wc = windows(ntt::Tune{kf, kr});
+            if (wc.empty() || wc == wdef) continue;
+            const double td = time_plan(def), tc = time_plan(ntt::Tune{kf, kr});
+            if (td < 0 || tc < 0) {
+                ntt::set_tuned((uint32_t)nBits, (uint32_t)nBitsExt, nCols, def);
                 cleanup();
                 return set_err(B200_ECUDA, "autotune run failed");
             }
-            if (ms_best < best) {
-                best = ms_best;
+            if (td < best && bt.kfirst == def.kfirst && bt.krest == def.krest) best = td;
+            const double ratio = tc / td;
+            if (ratio < 0.97 && ratio < best_ratio) {
+                best_ratio = ratio;
                 bt = ntt::Tune{kf, kr};
+                best = tc;
             }
         }
     }
+    if (best > 1e29) best = time_plan(bt);  // every candidate had the default's windows
     ntt::set_tuned((uint32_t)nBits, (uint32_t)nBitsExt, nCols, bt);
     cleanup();
     if (best_ms) *best_ms = best;
