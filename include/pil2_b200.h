@@ -312,6 +312,29 @@ int b200_commit_packed_device(uint64_t *root_host, uint64_t *d_lde, uint64_t *d_
                               uint64_t words_per_row, const uint32_t *col_bits, uint64_t nBits, uint64_t nBitsExt,
                               uint64_t nCols, uint64_t arity, uint64_t *d_scratch, void *stream);
 
+/* ---- streaming slot commit of a bit-packed witness (commit_witness_streaming & co.,
+ * starks_api.hpp:212-217; streamCommitPacked, goldilocks/src/stream_commit.cuh) ----
+ * Columns are extended and absorbed RATE = 12 at a time into the row sponge (W16, arity 4), so
+ * the NExt x nCols LDE is never materialised; the root equals the ordinary commit's.  nCols must
+ * be 1..64 and nBitsExt > nBits (stream_commit_slot_bytes returns 0 otherwise).  The reference
+ * entry points hash with Poseidon1 only (set_hash_family(1), else -15), own their slots
+ * (configure_stream_commit_slots) and are synchronous.  Return codes: 0, -10 invalid shape or
+ * widths, -11 no slots, -12 slot index, -13 slot too small, -14 paused.  colWidths: host array
+ * of nCols u64 widths (1..64); packed: host rows of wordsPerRow u64 words. */
+uint64_t stream_commit_slot_bytes(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t wordsPerRow);
+void configure_stream_commit_slots(void *d_buffers, uint64_t nSlots, uint64_t slotBytes);
+uint64_t get_stream_commit_slots(void *d_buffers);
+uint64_t get_stream_commit_floor(void *d_buffers);
+int64_t commit_witness_streaming(void *d_buffers, uint64_t slotIdx, uint64_t airgroupId, uint64_t airId, void *packed,
+                                 uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t wordsPerRow,
+                                 void *colWidths, void *root);
+void stream_commit_pause(void);
+/* Native form: caller-owned device slot of slot_words words (>= stream_commit_slot_bytes / 8),
+ * the native hash family (b200_set_native_hash_family); synchronous on `stream`. */
+int b200_stream_commit_packed(uint64_t *d_slot, uint64_t slot_words, const uint64_t *h_packed, uint64_t nBits,
+                              uint64_t nBitsExt, uint64_t nCols, uint64_t wordsPerRow, const uint64_t *colWidths,
+                              uint64_t *root, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -97,6 +97,14 @@ _SIGS = {
     "b200_autotune_load": (_i32, [ctypes.c_char_p]),
     "b200_packed_words_per_row": (_u64, [_vp, _u64]),
     "b200_commit_packed_device": (_i32, [_vp, _vp, _vp, _vp, _u64, _vp, _u64, _u64, _u64, _u64, _vp, _vp]),
+    # streaming slot commit
+    "stream_commit_slot_bytes": (_u64, [_u64, _u64, _u64, _u64]),
+    "configure_stream_commit_slots": (None, [_vp, _u64, _u64]),
+    "get_stream_commit_slots": (_u64, [_vp]),
+    "get_stream_commit_floor": (_u64, [_vp]),
+    "commit_witness_streaming": (ctypes.c_int64, [_vp, _u64, _u64, _u64, _vp, _u64, _u64, _u64, _u64, _vp, _vp]),
+    "stream_commit_pause": (None, []),
+    "b200_stream_commit_packed": (_i32, [_vp, _u64, _vp, _u64, _u64, _u64, _u64, _vp, _vp, _vp]),
 }
 
 _lib = None
@@ -418,3 +426,19 @@ def set_native_hash_family(family):
 
 def native_hash_family():
     return int(load().b200_native_hash_family())
+
+
+# ---------------------------------------------------------------- streaming slot commit ----
+def stream_commit_slot_bytes(nbits, nbits_ext, ncols, words_per_row):
+    return int(load().stream_commit_slot_bytes(nbits, nbits_ext, ncols, words_per_row))
+
+
+def stream_commit_packed(d_slot, slot_words, packed, col_bits, nbits, nbits_ext, stream=None):
+    """Native streaming commit of host packed rows (N, words_per_row); returns the root."""
+    packed = np.ascontiguousarray(packed, dtype=np.uint64)
+    widths = np.ascontiguousarray(col_bits, dtype=np.uint64)
+    root = np.zeros(4, dtype=np.uint64)
+    _check(load().b200_stream_commit_packed(_ptr(d_slot), slot_words, packed.ctypes.data, nbits, nbits_ext,
+                                            widths.size, packed.shape[1], widths.ctypes.data, root.ctypes.data,
+                                            _stream(stream)))
+    return root

@@ -180,6 +180,48 @@ __device__ __forceinline__ uint64_t sub(uint64_t a, uint64_t b)
     return mk64(s0, s1);
 }
 
+// a - b where b < p (canonical): one borrow fix-up suffices (a second borrow would need b > p)
+__device__ __forceinline__ uint64_t sub_c(uint64_t a, uint64_t b)
+{
+    uint32_t s0, s1, c;
+    asm("sub.cc.u32  %0, %3, %5;\n\t"
+        "subc.cc.u32 %1, %4, %6;\n\t"
+        "subc.u32    %2, 0, 0;\n\t"
+        : "=r"(s0), "=r"(s1), "=r"(c)
+        : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
+    asm("sub.cc.u32  %0, %0, %2;\n\t"
+        "subc.u32    %1, %1, 0;\n\t"
+        : "+r"(s0), "+r"(s1)
+        : "r"(c));
+    return mk64(s0, s1);
+}
+
+// x * 2^S mod p for 0 < S < 96 by shifts: x << S spans at most three 32-bit words placed at word
+// offset S/32; the 128-bit reduction folds it, and a word that lands at 2^128 is folded with
+// 2^128 = -2^32 (mod p).  Multiplication by the radix-16 roots of unity (powers of w_16 = 2^12)
+// costs three shifts and one reduction instead of four wide products.
+template <int S>
+__device__ __forceinline__ uint64_t mul_pow2(uint64_t x)
+{
+    static_assert(S > 0 && S < 96, "shift out of range");
+    constexpr int Q = S / 32, T = S % 32;
+    const uint32_t x0 = lo32(x), x1 = hi32(x);
+    uint32_t u0, u1, u2;
+    if (T == 0) {
+        u0 = x0;
+        u1 = x1;
+        u2 = 0;
+    } else {
+        u0 = x0 << T;
+        u1 = __funnelshift_l(x0, x1, T);
+        u2 = x1 >> (32 - T);
+    }
+    if (Q == 0) return reduce128(u0, u1, u2, 0u);
+    if (Q == 1) return reduce128(0u, u0, u1, u2);
+    const uint64_t y = reduce128(0u, 0u, u0, u1);
+    return sub_c(y, (uint64_t)u2 << 32);  // u2 < 2^T <= 2^31: u2 * 2^32 < p
+}
+
 // x^7 = x^3 * x^4, the Poseidon2 S-box (poseidon2_goldilocks.hpp:147-155)
 __device__ __forceinline__ uint64_t pow7(uint64_t x)
 {

@@ -148,20 +148,12 @@ inline uint64_t tree_num_elements(uint64_t nrows, uint64_t arity)
     return total * 4;
 }
 
-// Leaf digests and every level up to the root, on `stream`.
+// Every tree level above `nrows` leaf digests already at the start of d_tree, on `stream`.
 template <int W, int FAM = 2>
-cudaError_t build_tree(uint64_t *d_tree, const uint64_t *d_src, uint64_t rs, uint64_t cs, uint64_t ncols,
-                       uint64_t nrows, cudaStream_t stream)
+cudaError_t build_levels(uint64_t *d_tree, uint64_t nrows, cudaStream_t stream)
 {
     constexpr uint64_t ARITY = W / 4;
-    if (nrows == 0) return cudaSuccess;
     const unsigned tpb = TPB;
-    {
-        prof::Scope ps(prof::LEAF_HASH, stream);
-        leaf_hash_kernel<W, FAM><<<(unsigned)((nrows + tpb - 1) / tpb), tpb, 0, stream>>>(d_tree, d_src, rs, cs, ncols,
-                                                                                       nrows);
-        prof::count();
-    }
     prof::Scope ps(prof::TREE_LEVELS, stream);
     uint64_t pending = nrows, base = 0;
     while (pending > 1) {
@@ -175,6 +167,22 @@ cudaError_t build_tree(uint64_t *d_tree, const uint64_t *d_src, uint64_t rs, uin
         pending = parents;
     }
     return cudaGetLastError();
+}
+
+// Leaf digests and every level up to the root, on `stream`.
+template <int W, int FAM = 2>
+cudaError_t build_tree(uint64_t *d_tree, const uint64_t *d_src, uint64_t rs, uint64_t cs, uint64_t ncols,
+                       uint64_t nrows, cudaStream_t stream)
+{
+    if (nrows == 0) return cudaSuccess;
+    const unsigned tpb = TPB;
+    {
+        prof::Scope ps(prof::LEAF_HASH, stream);
+        leaf_hash_kernel<W, FAM><<<(unsigned)((nrows + tpb - 1) / tpb), tpb, 0, stream>>>(d_tree, d_src, rs, cs, ncols,
+                                                                                       nrows);
+        prof::count();
+    }
+    return build_levels<W, FAM>(d_tree, nrows, stream);
 }
 
 // family: 1 = Poseidon1, otherwise Poseidon2; W = 4 * arity (MerkleTreeGL::merkelize)

@@ -74,7 +74,7 @@ __device__ __forceinline__ uint64_t big_twiddle(uint64_t e, bool inv)
 // The 2^k-point transform of a window is split into phases of r <= 4 stages.  In a
 // phase each thread takes the 2^r elements of one sub-transform (mid = hi|j<<pb|lo_m),
 // applies the phase twiddle w_{2^(pb+r)}^(bitrev_r(j)*lo_m) (before, DIT; after, DIF),
-// and runs the r radix-2 stages in registers with the compile-time roots w_2..w_16;
+// and runs the r radix-2 stages in registers (roots w_2..w_16 are powers of 2^12: shifts);
 // shared memory is touched once per phase instead of once per stage.  Shared memory is
 // padded by one word per 16 (index i -> i + i/16) so that a thread's 16 contiguous
 // elements of the first phase sit in different banks from its neighbours'.
@@ -85,23 +85,27 @@ __device__ uint64_t g_ntt_w4096_inv[4096];  // w_4096^-i
 
 __device__ __forceinline__ uint32_t pad16(uint32_t i) { return i + (i >> 4); }
 
-// roots of unity of order <= 16 as compile-time constants: w_{2^(u+1)}^e (inverse if INV)
-template <bool INV>
-__device__ __forceinline__ uint64_t small_root(int u, int e)
+// x * w_16^idx = x * 2^(12 idx) (idx constant once the butterfly loops are unrolled)
+__device__ __forceinline__ uint64_t mul_root16(uint64_t x, int idx)
 {
-    // w_16 = W[4] = 2^12 (goldilocks_base_field.cpp:16): F[e] = w_16^e, I[e] = w_16^-e mod p
-    constexpr uint64_t F[8] = {1ull, 4096ull, 16777216ull, 68719476736ull, 281474976710656ull,
-                               1152921504606846976ull, 1099511627520ull, 4503599626321920ull};
-    constexpr uint64_t I[8] = {1ull, 18442240469788262401ull, 18446742969902956801ull, 17293822564807737345ull,
-                               18446462594437873665ull, 18446744000695107585ull, 18446744069397807105ull,
-                               18446744069414580225ull};
-    const int idx = e << (3 - u);  // w_{2^(u+1)}^e = w_16^(e * 2^(3-u))
-    return INV ? I[idx] : F[idx];
+    switch (idx) {
+    case 1: return gl::mul_pow2<12>(x);
+    case 2: return gl::mul_pow2<24>(x);
+    case 3: return gl::mul_pow2<36>(x);
+    case 4: return gl::mul_pow2<48>(x);
+    case 5: return gl::mul_pow2<60>(x);
+    case 6: return gl::mul_pow2<72>(x);
+    case 7: return gl::mul_pow2<84>(x);
+    default: return x;
+    }
 }
 
+// Forward radix-2^R DIT network.  The twiddled operand is made canonical, so the butterfly's add
+// and subtract each need one carry fold; the roots w_16^idx = 2^(12 idx) are shift multiplies.
 template <int R, bool INV>
 __device__ __forceinline__ void radix_dit(uint64_t (&v)[16])
 {
+    static_assert(!INV, "the DIT network runs forward transforms");
 #pragma unroll
     for (int u = 0; u < R; u++) {
         const int h = 1 << u;
@@ -110,17 +114,21 @@ __device__ __forceinline__ void radix_dit(uint64_t (&v)[16])
             if (j & h) continue;
             const int e = j & (h - 1);
             uint64_t x = v[j + h];
-            if (e) x = gl::mul(x, small_root<INV>(u, e));
+            if (e) x = mul_root16(x, e << (3 - u));
+            x = gl::canon(x);
             const uint64_t y = v[j];
-            v[j] = gl::add(y, x);
-            v[j + h] = gl::sub(y, x);
+            v[j] = gl::add_c(y, x);
+            v[j + h] = gl::sub_c(y, x);
         }
     }
 }
 
+// Inverse radix-2^R DIF network.  w_16^-idx = -2^(96 - 12 idx), so a twiddled difference is
+// (x - y) * 2^(96 - 12 idx); the untwiddled ones use the canonical operand's single-fold forms.
 template <int R, bool INV>
 __device__ __forceinline__ void radix_dif(uint64_t (&v)[16])
 {
+    static_assert(INV, "the DIF network runs inverse transforms");
 #pragma unroll
     for (int u = R - 1; u >= 0; u--) {
         const int h = 1 << u;
@@ -128,11 +136,12 @@ __device__ __forceinline__ void radix_dif(uint64_t (&v)[16])
         for (int j = 0; j < (1 << R); j++) {
             if (j & h) continue;
             const int e = j & (h - 1);
-            const uint64_t y = v[j], x = v[j + h];
-            v[j] = gl::add(y, x);
-            uint64_t d = gl::sub(y, x);
-            if (e) d = gl::mul(d, small_root<INV>(u, e));
-            v[j + h] = d;
+            const uint64_t y = v[j], x = gl::canon(v[j + h]);
+            v[j] = gl::add_c(y, x);
+            if (e)
+                v[j + h] = mul_root16(gl::sub(x, y), 8 - (e << (3 - u)));
+            else
+                v[j + h] = gl::sub_c(y, x);
         }
     }
 }

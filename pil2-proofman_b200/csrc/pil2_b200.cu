@@ -377,7 +377,19 @@ struct CommitBuffers {
     std::vector<Slot> slots;
     uint64_t seq = 0;
     std::atomic<int> error{0};
+    // end event of the most recently issued commit: the next commit's kernels wait for it, so
+    // commits run one after another on the GPU while the next trace's H2D overlaps them (two
+    // commits interleaving would finish together and leave the GPU idle during both next copies)
+    cudaEvent_t last_end = nullptr;
+    // streaming slot commits (configure_stream_commit_slots): one device block of n slots
+    uint64_t *sc_base = nullptr;
+    uint64_t sc_slot_bytes = 0;
+    std::vector<cudaStream_t> sc_streams;
+    std::atomic<int> sc_quiesced{0}, sc_inflight{0};
 };
+
+// the buffers whose streaming slots stream_commit_pause quiesces (the last configured)
+static std::atomic<CommitBuffers *> g_stream_buffers{nullptr};
 
 static int grow(uint64_t *&p, uint64_t &cap, uint64_t words)
 {
@@ -437,6 +449,13 @@ extern "C" void free_device_buffers(void *d_buffers)
     auto *b = (CommitBuffers *)d_buffers;
     if (!b) return;
     for (auto &s : b->slots) slot_destroy(s);
+    for (cudaStream_t t : b->sc_streams) {
+        cudaStreamSynchronize(t);
+        cudaStreamDestroy(t);
+    }
+    if (b->sc_base) cudaFree(b->sc_base);
+    CommitBuffers *expect = b;
+    g_stream_buffers.compare_exchange_strong(expect, nullptr);
     delete b;
 }
 
@@ -462,6 +481,7 @@ extern "C" uint64_t gen_device_streams(void *d_buffers, uint64_t n_streams, uint
     cudaSetDevice(b->device);
     if (merkleTreeArity) b->arity = (uint32_t)merkleTreeArity;
     for (auto &s : b->slots) harvest(s);
+    b->last_end = nullptr;  // every slot is idle; slots may be destroyed below
     while (b->slots.size() > n_streams) {
         slot_destroy(b->slots.back());
         b->slots.pop_back();
@@ -489,13 +509,14 @@ static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_
     if (N * nCols)
         CK(cudaMemcpyAsync(s.d_trace, trace, N * nCols * 8, cudaMemcpyHostToDevice, s.stream), "trace H2D");
     CK(cudaEventRecord(s.h2d_done, s.stream), "event");
+    if (b->last_end && b->last_end != s.end) CK(cudaStreamWaitEvent(s.stream, b->last_end, 0), "order commits");
     CK(ntt::lde(s.d_lde, s.d_trace, true, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, s.d_scratch, s.stream),
        "lde");
     CK(merkle::build_tree_arity(arity, s.d_tree, s.d_lde, 1, NExt, nCols, NExt, s.stream, g_hash_family.load()),
        "merkletree");
     CK(cudaMemcpyAsync(s.h_root, s.d_tree + tsz - 4, 32, cudaMemcpyDeviceToHost, s.stream), "root D2H");
     CK(cudaEventRecord(s.end, s.stream), "event");
-    (void)b;
+    b->last_end = s.end;
     return B200_OK;
 }
 
@@ -979,4 +1000,158 @@ extern "C" int b200_commit_packed_device(uint64_t *root_host, uint64_t *d_lde, u
         CK(cudaStreamSynchronize(s), "sync");
     }
     return B200_OK;
+}
+
+// ------------------------------------------------------ streaming slot commit ----
+#include "stream.cuh"
+
+// Widths -> the slot's width and bit-offset tables (host staging of 2 x 64 words).
+static int stream_tables(uint64_t *tab, const uint64_t *colWidths, uint64_t nCols, uint64_t wordsPerRow)
+{
+    uint64_t off = 0;
+    for (uint64_t c = 0; c < nCols; c++) {
+        if (colWidths[c] < 1 || colWidths[c] > 64) return set_err(B200_EINVAL, "column width outside 1..64");
+        tab[c] = colWidths[c];
+        tab[stream::MAX_COLS + c] = off;
+        off += colWidths[c];
+    }
+    if (off > 64 * wordsPerRow) return set_err(B200_EINVAL, "wordsPerRow too small for the column widths");
+    return B200_OK;
+}
+
+// One streaming commit on a slot: H2D of the packed rows and the tables, the chunked LDE +
+// absorb, the tree levels, the root D2H; synchronous.
+static int stream_commit_on(uint64_t *slot, uint64_t slot_words, cudaStream_t s, const void *h_packed,
+                            uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t wordsPerRow,
+                            const uint64_t *colWidths, uint64_t *root, int family)
+{
+    if (nCols == 0 || nCols > stream::MAX_COLS || nBitsExt <= nBits || wordsPerRow == 0 || !colWidths || !h_packed ||
+        !root)
+        return set_err(B200_EINVAL, "streaming commit: nCols must be 1..64, nBitsExt > nBits, buffers non-null");
+    int rc = check_shape(nBits, nBitsExt, nCols, 4);
+    if (rc) return rc;
+    const stream::Layout l = stream::layout(nBits, nBitsExt, wordsPerRow);
+    if (l.total > slot_words) return set_err(B200_EINVAL, "slot too small for this shape");
+    uint64_t tab[2 * stream::MAX_COLS] = {0};
+    if ((rc = stream_tables(tab, colWidths, nCols, wordsPerRow))) return rc;
+    if ((rc = ensure_init_current())) return rc;
+    const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
+    CK(cudaMemcpyAsync(slot + l.widths, tab, sizeof(tab), cudaMemcpyHostToDevice, s), "tables H2D");
+    CK(cudaMemcpyAsync(slot + l.packed, h_packed, N * wordsPerRow * 8, cudaMemcpyHostToDevice, s), "packed H2D");
+    CK(family == 1 ? stream::run<1>(slot, l, nBits, nBitsExt, nCols, wordsPerRow, s)
+                   : stream::run<2>(slot, l, nBits, nBitsExt, nCols, wordsPerRow, s),
+       "streaming commit");
+    const uint64_t tsz = merkle::tree_num_elements(NExt, 4);
+    CK(cudaMemcpyAsync(root, slot + l.tree + tsz - 4, 32, cudaMemcpyDeviceToHost, s), "root D2H");
+    CK(cudaStreamSynchronize(s), "sync");
+    return B200_OK;
+}
+
+extern "C" uint64_t stream_commit_slot_bytes(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t wordsPerRow)
+{
+    if (nCols == 0 || nCols > stream::MAX_COLS || nBitsExt <= nBits || wordsPerRow == 0 || nBitsExt > NTT_TWLG) return 0;
+    return stream::layout(nBits, nBitsExt, wordsPerRow).total * 8;
+}
+
+extern "C" void configure_stream_commit_slots(void *d_buffers, uint64_t nSlots, uint64_t slotBytes)
+{
+    auto *b = (CommitBuffers *)d_buffers;
+    if (!b) return;
+    std::lock_guard<std::mutex> lk(b->mu);
+    cudaSetDevice(b->device);
+    for (cudaStream_t t : b->sc_streams) {
+        cudaStreamSynchronize(t);
+        cudaStreamDestroy(t);
+    }
+    b->sc_streams.clear();
+    if (b->sc_base) cudaFree(b->sc_base);
+    b->sc_base = nullptr;
+    b->sc_slot_bytes = 0;
+    if (nSlots == 0 || slotBytes == 0) return;
+    slotBytes = (slotBytes + 255) & ~255ull;
+    if (cudaMalloc((void **)&b->sc_base, nSlots * slotBytes) != cudaSuccess) {
+        cudaGetLastError();
+        b->sc_base = nullptr;
+        b->error = set_err(B200_ENOMEM, "configure_stream_commit_slots: cudaMalloc");
+        return;
+    }
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);  // lo = numerically largest = lowest priority
+    for (uint64_t i = 0; i < nSlots; i++) {
+        cudaStream_t t;
+        if (cudaStreamCreateWithPriority(&t, cudaStreamNonBlocking, lo) != cudaSuccess) {
+            b->error = set_err(B200_ECUDA, "configure_stream_commit_slots: stream");
+            return;
+        }
+        b->sc_streams.push_back(t);
+    }
+    b->sc_slot_bytes = slotBytes;
+    b->sc_quiesced.store(0);
+    g_stream_buffers.store(b);
+}
+
+extern "C" uint64_t get_stream_commit_slots(void *d_buffers)
+{
+    auto *b = (CommitBuffers *)d_buffers;
+    return b ? b->sc_streams.size() : 0;
+}
+
+// The reference carves its slots out of its unified buffer and reports where they start; this
+// library allocates them on their own, so the offset within that allocation is 0.
+extern "C" uint64_t get_stream_commit_floor(void *d_buffers)
+{
+    auto *b = (CommitBuffers *)d_buffers;
+    if (!b) return UINT64_MAX;
+    return 0;
+}
+
+// Return codes follow commit_witness_streaming (api/starks_api.cu:2290-2348): 0 ok, -11 no slots,
+// -12 slot index out of range, -13 slot too small for the shape, -14 quiesced by
+// stream_commit_pause, -15 hash family is not Poseidon1; -10 invalid shape or widths.  The
+// indexed (instruction-table) witness is not supported (-16).
+extern "C" int64_t commit_witness_streaming(void *d_buffers, uint64_t slotIdx, uint64_t airgroupId, uint64_t airId,
+                                            void *packed, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols,
+                                            uint64_t wordsPerRow, void *colWidths, void *root)
+{
+    (void)airgroupId;
+    (void)airId;
+    auto *b = (CommitBuffers *)d_buffers;
+    if (!b || b->sc_streams.empty()) return -11;
+    if (slotIdx >= b->sc_streams.size()) return -12;
+    if (g_hash_family.load() != 1) return -15;
+    if (stream_commit_slot_bytes(nBits, nBitsExt, nCols, wordsPerRow) == 0) return -10;
+    if (stream::layout(nBits, nBitsExt, wordsPerRow).total * 8 > b->sc_slot_bytes) return -13;
+    if (b->sc_quiesced.load()) return -14;
+    b->sc_inflight++;
+    if (b->sc_quiesced.load()) {
+        b->sc_inflight--;
+        return -14;
+    }
+    cudaSetDevice(b->device);
+    uint64_t *slot = b->sc_base + slotIdx * (b->sc_slot_bytes / 8);
+    int rc = stream_commit_on(slot, b->sc_slot_bytes / 8, b->sc_streams[slotIdx], packed, nBits, nBitsExt, nCols,
+                              wordsPerRow, (const uint64_t *)colWidths, (uint64_t *)root, 1);
+    b->sc_inflight--;
+    return rc == B200_OK ? 0 : -10;
+}
+
+// Reject new slot commits and wait (bounded, about 2 s) for the running ones to finish.
+
+extern "C" void stream_commit_pause(void)
+{
+    CommitBuffers *b = g_stream_buffers.load();
+    if (!b) return;
+    b->sc_quiesced.store(1);
+    for (int i = 0; i < 4000 && b->sc_inflight.load() != 0; i++) std::this_thread::sleep_for(std::chrono::microseconds(500));
+}
+
+// Native form with caller-owned device slot memory and the native hash family (no reference
+// counterpart; the reference entry above is Poseidon1-only and owns its slots).
+extern "C" int b200_stream_commit_packed(uint64_t *d_slot, uint64_t slot_words, const uint64_t *h_packed,
+                                         uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t wordsPerRow,
+                                         const uint64_t *colWidths, uint64_t *root, void *stream)
+{
+    if (!d_slot) return set_err(B200_EINVAL, "null slot");
+    return stream_commit_on(d_slot, slot_words, (cudaStream_t)stream, h_packed, nBits, nBitsExt, nCols, wordsPerRow,
+                            colWidths, root, g_native_family.load());
 }

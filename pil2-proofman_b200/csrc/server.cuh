@@ -54,6 +54,7 @@ class Server {
     bool stop = false;
     std::thread worker;
     cudaMemPool_t pool = nullptr;
+    cudaEvent_t last_done = nullptr;  // completion event of the most recently admitted request
 
     int start(int dev, uint64_t budget_bytes, uint32_t slots)
     {
@@ -182,6 +183,9 @@ class Server {
         if (!rc && r->words_trace &&
             cudaMemcpyAsync(r->d_trace, r->trace, 8 * r->words_trace, cudaMemcpyHostToDevice, s) != cudaSuccess)
             rc = B200_ECUDA;
+        // kernels of admitted requests run in admission order (the H2D above overlaps the previous
+        // request's kernels); interleaved requests would each take longer and finish together
+        if (!rc && last_done) cudaStreamWaitEvent(s, last_done, 0);
         if (!rc) rc = commit_device_fam(nullptr, r->d_lde, r->d_tree, r->d_trace, 1, r->nBits, r->nBitsExt, r->nCols,
                                         r->arity, r->d_scratch, s, 2);
         if (!rc && cudaMemcpyAsync(r->h_root, r->d_tree + r->words_tree - 4, 32, cudaMemcpyDeviceToHost, s) !=
@@ -193,6 +197,7 @@ class Server {
             cudaFreeAsync(r->d_scratch, s);
             r->d_trace = r->d_scratch = nullptr;
             if (cudaEventRecord(r->done, s) != cudaSuccess) rc = B200_ECUDA;
+            else last_done = r->done;
         }
         if (rc) {
             free_buffers(r, s);
