@@ -76,8 +76,8 @@ def test_stream_commit_rejects(pkg, torch_cuda):
     with pytest.raises(pkg.B200Error):
         pkg.stream_commit_packed(small, nbytes // 16, packed, bits, 6, 7)
     slot = torch.zeros(nbytes // 8, dtype=torch.int64, device="cuda")
-    with pytest.raises(pkg.B200Error):  # widths wider than the packed rows
-        pkg.stream_commit_packed(slot, nbytes // 8, packed, [30, 30, 40], 6, 7)
+    with pytest.raises(pkg.B200Error):  # 158 bits of widths do not fit the 2 packed words per row
+        pkg.stream_commit_packed(slot, nbytes // 8, packed, [64, 64, 30], 6, 7)
     # the reference entry refuses a Poseidon2 process (this test process uses family 2)
     pkg.set_hash_family(2)
     bufs = pkg.DeviceBuffers(arity=4, n_streams=1)
