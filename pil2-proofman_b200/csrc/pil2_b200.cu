@@ -361,7 +361,9 @@ extern "C" void b200_stark_shape_free(void *shape) { delete (B200StarkShape *)sh
 // One stream slot: its own device buffers, kept resident after the commit.
 struct Slot {
     cudaStream_t stream = nullptr;
+    cudaStream_t copy = nullptr;  // host-to-device copies of the trace, block by block
     cudaEvent_t h2d_done = nullptr, end = nullptr;
+    std::vector<cudaEvent_t> blocks;  // one per column block: that block's copy has landed
     uint64_t *d_trace = nullptr, *d_scratch = nullptr, *d_lde = nullptr, *d_tree = nullptr;
     uint64_t cap_trace = 0, cap_scratch = 0, cap_lde = 0, cap_tree = 0;
     uint64_t *h_root = nullptr;  // pinned 4 words
@@ -405,6 +407,7 @@ static int grow(uint64_t *&p, uint64_t &cap, uint64_t words)
 static int slot_create(Slot &s)
 {
     CK(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "stream");
+    CK(cudaStreamCreateWithFlags(&s.copy, cudaStreamNonBlocking), "stream");
     CK(cudaEventCreateWithFlags(&s.h2d_done, cudaEventDisableTiming), "event");
     CK(cudaEventCreateWithFlags(&s.end, cudaEventDisableTiming), "event");
     CK(cudaMallocHost((void **)&s.h_root, 32), "pinned root");
@@ -414,12 +417,15 @@ static int slot_create(Slot &s)
 static void slot_destroy(Slot &s)
 {
     if (s.stream) cudaStreamSynchronize(s.stream);
+    if (s.copy) cudaStreamSynchronize(s.copy);
+    for (cudaEvent_t e : s.blocks) cudaEventDestroy(e);
     for (uint64_t *p : {s.d_trace, s.d_scratch, s.d_lde, s.d_tree})
         if (p) cudaFree(p);
     if (s.h_root) cudaFreeHost(s.h_root);
     if (s.h2d_done) cudaEventDestroy(s.h2d_done);
     if (s.end) cudaEventDestroy(s.end);
     if (s.stream) cudaStreamDestroy(s.stream);
+    if (s.copy) cudaStreamDestroy(s.copy);
     s = Slot{};
 }
 
@@ -496,7 +502,19 @@ extern "C" uint64_t gen_device_streams(void *d_buffers, uint64_t n_streams, uint
     return b->slots.size();
 }
 
-// Enqueue H2D + LDE + tree + root D2H for a row-major host trace on a slot.
+// Column blocks of the pipelined commit: 64 columns (512-byte row segments, which a 2-D copy
+// moves at full PCIe rate) when the trace is large enough for the overlap to matter.
+static uint64_t commit_block_cols(uint64_t nBits, uint64_t nCols)
+{
+    return (nBits >= 16 && nCols >= 128) ? 64 : nCols;
+}
+
+// Enqueue H2D + LDE + tree + root D2H for a row-major host trace on a slot.  The trace crosses
+// PCIe in column blocks on the slot's copy stream (a 2-D copy each, into a row-major N x B block
+// of d_trace); the compute stream transposes and extends each block as soon as it has landed, so
+// the LDE of a block overlaps the copy of the next, then hashes the rows once every column is
+// extended.  The compute stream also waits for the previously issued commit to end (see
+// CommitBuffers::last_end); the copy stream only for this slot's previous commit.
 static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_t nBits, uint64_t nBitsExt,
                        uint64_t nCols, uint64_t arity)
 {
@@ -506,12 +524,47 @@ static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_
     if ((rc = grow(s.d_trace, s.cap_trace, N * nCols)) || (rc = grow(s.d_scratch, s.cap_scratch, N * nCols)) ||
         (rc = grow(s.d_lde, s.cap_lde, NExt * nCols)) || (rc = grow(s.d_tree, s.cap_tree, tsz)))
         return rc;
-    if (N * nCols)
-        CK(cudaMemcpyAsync(s.d_trace, trace, N * nCols * 8, cudaMemcpyHostToDevice, s.stream), "trace H2D");
-    CK(cudaEventRecord(s.h2d_done, s.stream), "event");
+    const uint64_t B = nCols ? commit_block_cols(nBits, nCols) : 1;
+    const uint64_t nblk = nCols ? (nCols + B - 1) / B : 0;
+    while (s.blocks.size() < nblk) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        s.blocks.push_back(e);
+    }
+    // the copy may overwrite d_trace once this slot's previous commit has consumed it
+    CK(cudaStreamWaitEvent(s.copy, s.end, 0), "slot reuse");
+    for (uint64_t k = 0; k < nblk; k++) {
+        const uint64_t c0 = k * B, cb = (nCols - c0) < B ? (nCols - c0) : B;
+        if (cb == nCols)
+            CK(cudaMemcpyAsync(s.d_trace, trace, N * nCols * 8, cudaMemcpyHostToDevice, s.copy), "trace H2D");
+        else
+            CK(cudaMemcpy2DAsync(s.d_trace + c0 * N, cb * 8, trace + c0, nCols * 8, cb * 8, N, cudaMemcpyHostToDevice,
+                                 s.copy),
+               "trace block H2D");
+        CK(cudaEventRecord(s.blocks[k], s.copy), "event");
+    }
+    CK(cudaEventRecord(s.h2d_done, s.copy), "event");
     if (b->last_end && b->last_end != s.end) CK(cudaStreamWaitEvent(s.stream, b->last_end, 0), "order commits");
-    CK(ntt::lde(s.d_lde, s.d_trace, true, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, s.d_scratch, s.stream),
-       "lde");
+    for (uint64_t k = 0; k < nblk; k++) {
+        const uint64_t c0 = k * B, cb = (nCols - c0) < B ? (nCols - c0) : B;
+        CK(cudaStreamWaitEvent(s.stream, s.blocks[k], 0), "block landed");
+        if (cb == nCols) {
+            CK(ntt::lde(s.d_lde, s.d_trace, true, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, s.d_scratch, s.stream),
+               "lde");
+        } else {
+            {
+                prof::Scope ps(prof::TRANSPOSE, s.stream);
+                dim3 grid((unsigned)((N + 31) / 32), (unsigned)((cb + 31) / 32));
+                ntt::transpose_kernel<<<grid, dim3(32, 8), 0, s.stream>>>(s.d_scratch + c0 * N, s.d_trace + c0 * N, N,
+                                                                          cb, N);
+                prof::count();
+                CK(cudaGetLastError(), "transpose");
+            }
+            CK(ntt::lde(s.d_lde + c0 * NExt, s.d_scratch + c0 * N, false, (uint32_t)nBits, (uint32_t)nBitsExt, cb,
+                        s.d_scratch + c0 * N, s.stream),
+               "lde");
+        }
+    }
     CK(merkle::build_tree_arity(arity, s.d_tree, s.d_lde, 1, NExt, nCols, NExt, s.stream, g_hash_family.load()),
        "merkletree");
     CK(cudaMemcpyAsync(s.h_root, s.d_tree + tsz - 4, 32, cudaMemcpyDeviceToHost, s.stream), "root D2H");
