@@ -335,6 +335,28 @@ int b200_stream_commit_packed(uint64_t *d_slot, uint64_t slot_words, const uint6
                               uint64_t nBitsExt, uint64_t nCols, uint64_t wordsPerRow, const uint64_t *colWidths,
                               uint64_t *root, void *stream);
 
+/* ---- indexed witness (instruction table; unpack_indexed, starks_gpu.cu:125-185) ----
+ * A row is a leading instruction index (index_bits) followed by the runtime columns; columns with
+ * col_source[c] = 1 are read from entry `index` of the instruction table (words_per_entry words
+ * per entry; an index past the table selects entry 0).  register_instruction_table
+ * (starks_api.hpp:192) hands the table to the buffers object; b200_register_indexed_air stands in
+ * for the setup's PackedInfo (which columns come from the table, the index width).  With both
+ * registered for (airgroupId, airId), commit_witness_streaming commits that AIR's indexed rows
+ * (-16 when the table is missing). */
+void register_instruction_table(void *d_buffers, uint64_t airgroupId, uint64_t airId, uint64_t *table,
+                                uint64_t num_entries, uint64_t words_per_entry);
+int b200_register_indexed_air(void *d_buffers, uint64_t airgroupId, uint64_t airId, uint64_t nCols,
+                              const uint8_t *col_source, uint64_t index_bits);
+int b200_commit_indexed_device(uint64_t *root_host, uint64_t *d_lde, uint64_t *d_tree, const uint64_t *d_rows,
+                               uint64_t words_per_row, const uint64_t *d_table, uint64_t num_entries,
+                               uint64_t words_per_entry, uint64_t index_bits, const uint64_t *col_bits,
+                               const uint8_t *col_source, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols,
+                               uint64_t arity, uint64_t *d_scratch, void *stream);
+int b200_stream_commit_indexed(uint64_t *d_slot, uint64_t slot_words, const uint64_t *h_rows, uint64_t nBits,
+                               uint64_t nBitsExt, uint64_t nCols, uint64_t words_per_row, const uint64_t *col_bits,
+                               const uint8_t *col_source, uint64_t index_bits, const uint64_t *d_table,
+                               uint64_t num_entries, uint64_t words_per_entry, uint64_t *root, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -105,6 +105,13 @@ _SIGS = {
     "commit_witness_streaming": (ctypes.c_int64, [_vp, _u64, _u64, _u64, _vp, _u64, _u64, _u64, _u64, _vp, _vp]),
     "stream_commit_pause": (None, []),
     "b200_stream_commit_packed": (_i32, [_vp, _u64, _vp, _u64, _u64, _u64, _u64, _vp, _vp, _vp]),
+    # indexed witness
+    "register_instruction_table": (None, [_vp, _u64, _u64, _vp, _u64, _u64]),
+    "b200_register_indexed_air": (_i32, [_vp, _u64, _u64, _u64, _vp, _u64]),
+    "b200_commit_indexed_device": (_i32, [_vp, _vp, _vp, _vp, _u64, _vp, _u64, _u64, _u64, _vp, _vp, _u64, _u64,
+                                          _u64, _u64, _vp, _vp]),
+    "b200_stream_commit_indexed": (_i32, [_vp, _u64, _vp, _u64, _u64, _u64, _u64, _vp, _vp, _u64, _vp, _u64, _u64,
+                                          _vp, _vp]),
 }
 
 _lib = None
@@ -441,4 +448,51 @@ def stream_commit_packed(d_slot, slot_words, packed, col_bits, nbits, nbits_ext,
     _check(load().b200_stream_commit_packed(_ptr(d_slot), slot_words, packed.ctypes.data, nbits, nbits_ext,
                                             widths.size, packed.shape[1], widths.ctypes.data, root.ctypes.data,
                                             _stream(stream)))
+    return root
+
+
+# ---------------------------------------------------------------- indexed witness ----
+def pack_indexed(runtime, index, index_bits, table_vals, col_bits, col_source):
+    """Host packer of an indexed witness.  runtime: (N, nRuntime) values of the source-0 columns in
+    column order; index: (N,) entry per row; table_vals: (E, nTable) values of the source-1 columns.
+    Returns (rows (N, words_per_row), table (E, words_per_entry))."""
+    col_bits = [int(b) for b in col_bits]
+    src = [int(x) for x in col_source]
+    rt_bits = [b for b, x in zip(col_bits, src) if not x]
+    tb_bits = [b for b, x in zip(col_bits, src) if x]
+    runtime = np.ascontiguousarray(runtime, dtype=np.uint64).reshape(len(index), len(rt_bits))
+    parts, widths = [], []
+    if index_bits:
+        parts.append(np.asarray(index, dtype=np.uint64)[:, None])
+        widths.append(index_bits)
+    parts.append(runtime)
+    widths += rt_bits
+    rows = pack_rows(np.concatenate(parts, axis=1), widths) if widths else np.zeros((len(index), 1), np.uint64)
+    table_vals = np.ascontiguousarray(table_vals, dtype=np.uint64).reshape(-1, len(tb_bits))
+    table = pack_rows(table_vals, tb_bits) if tb_bits else np.zeros((table_vals.shape[0], 0), np.uint64)
+    return rows, table
+
+
+def commit_indexed_device(d_lde, d_tree, d_rows, words_per_row, d_table, num_entries, words_per_entry, index_bits,
+                          col_bits, col_source, nbits, nbits_ext, arity, d_scratch, stream=None):
+    bits = np.ascontiguousarray(col_bits, dtype=np.uint64)
+    srcs = np.ascontiguousarray(col_source, dtype=np.uint8)
+    root = np.zeros(4, dtype=np.uint64)
+    _check(load().b200_commit_indexed_device(_ptr(root), _ptr(d_lde), _ptr(d_tree), _ptr(d_rows), words_per_row,
+                                             _ptr(d_table), num_entries, words_per_entry, index_bits,
+                                             bits.ctypes.data, srcs.ctypes.data, nbits, nbits_ext, bits.size, arity,
+                                             _ptr(d_scratch), _stream(stream)))
+    return root
+
+
+def stream_commit_indexed(d_slot, slot_words, rows, col_bits, col_source, index_bits, d_table, num_entries,
+                          words_per_entry, nbits, nbits_ext, stream=None):
+    rows = np.ascontiguousarray(rows, dtype=np.uint64)
+    bits = np.ascontiguousarray(col_bits, dtype=np.uint64)
+    srcs = np.ascontiguousarray(col_source, dtype=np.uint8)
+    root = np.zeros(4, dtype=np.uint64)
+    _check(load().b200_stream_commit_indexed(_ptr(d_slot), slot_words, rows.ctypes.data, nbits, nbits_ext, bits.size,
+                                             rows.shape[1], bits.ctypes.data, srcs.ctypes.data, index_bits,
+                                             _ptr(d_table), num_entries, words_per_entry, root.ctypes.data,
+                                             _stream(stream)))
     return root

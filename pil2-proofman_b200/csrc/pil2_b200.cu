@@ -278,7 +278,8 @@ extern "C" const char *b200_kernel_names(void)
 {
     return "pass16_kernel\ntranspose_kernel\nleaf_hash_kernel\nnode_kernel\npermute_kernel\nlde_rows_kernel\n"
            "fill_kernel\nimad_probe_kernel\ntranspose_grouped\npass_grouped\nleaf_persistent\n"
-           "node_grouped\ngather_roots\npass_fixed_kernel\nopenings_kernel\nunpack_kernel\n";
+           "node_grouped\ngather_roots\npass_fixed_kernel\nopenings_kernel\nunpack_kernel\nunpack_indexed_kernel\n"
+           "unpack_range_kernel\nabsorb_kernel\n";
 }
 
 // ------------------------------------------------------------ host-buffer API ----
@@ -388,6 +389,15 @@ struct CommitBuffers {
     uint64_t sc_slot_bytes = 0;
     std::vector<cudaStream_t> sc_streams;
     std::atomic<int> sc_quiesced{0}, sc_inflight{0};
+    // indexed witnesses per (airgroupId, airId): the row layout (b200_register_indexed_air, which
+    // stands in for the setup's PackedInfo) and the instruction table (register_instruction_table)
+    struct IndexedAir {
+        std::vector<uint8_t> col_source;
+        uint64_t index_bits = 0;
+        uint64_t *d_table = nullptr;
+        uint64_t num_entries = 0, words_per_entry = 0;
+    };
+    std::map<std::pair<uint64_t, uint64_t>, IndexedAir> indexed;
 };
 
 // the buffers whose streaming slots stream_commit_pause quiesces (the last configured)
@@ -460,6 +470,8 @@ extern "C" void free_device_buffers(void *d_buffers)
         cudaStreamDestroy(t);
     }
     if (b->sc_base) cudaFree(b->sc_base);
+    for (auto &kv : b->indexed)
+        if (kv.second.d_table) cudaFree(kv.second.d_table);
     CommitBuffers *expect = b;
     g_stream_buffers.compare_exchange_strong(expect, nullptr);
     delete b;
@@ -1072,11 +1084,37 @@ static int stream_tables(uint64_t *tab, const uint64_t *colWidths, uint64_t nCol
     return B200_OK;
 }
 
+// Indexed witness description for the host checks (col_source: 1 = table column).
+struct IndexedDesc {
+    const uint8_t *col_source;
+    uint64_t index_bits;
+    const uint64_t *d_table;
+    uint64_t num_entries, words_per_entry;
+};
+
+// col_info[c] = width | source << 32, and the row / table bit budgets checked
+static int indexed_info(uint64_t *info, const uint64_t *colWidths, uint64_t nCols, uint64_t wordsPerRow,
+                        const IndexedDesc &ix)
+{
+    if (ix.index_bits > 64) return set_err(B200_EINVAL, "index header wider than 64 bits");
+    uint64_t row_bits = ix.index_bits, tab_bits = 0;
+    for (uint64_t c = 0; c < nCols; c++) {
+        if (colWidths[c] < 1 || colWidths[c] > 64) return set_err(B200_EINVAL, "column width outside 1..64");
+        const uint64_t src = ix.col_source[c] ? 1 : 0;
+        info[c] = colWidths[c] | (src << 32);
+        (src ? tab_bits : row_bits) += colWidths[c];
+    }
+    if (row_bits > 64 * wordsPerRow) return set_err(B200_EINVAL, "wordsPerRow too small for the row columns");
+    if (tab_bits > 64 * ix.words_per_entry) return set_err(B200_EINVAL, "words_per_entry too small for the table columns");
+    if (tab_bits && (!ix.d_table || ix.num_entries == 0)) return set_err(B200_EINVAL, "table columns without a table");
+    return B200_OK;
+}
+
 // One streaming commit on a slot: H2D of the packed rows and the tables, the chunked LDE +
-// absorb, the tree levels, the root D2H; synchronous.
+// absorb, the tree levels, the root D2H; synchronous.  ix: indexed witness, or null.
 static int stream_commit_on(uint64_t *slot, uint64_t slot_words, cudaStream_t s, const void *h_packed,
                             uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t wordsPerRow,
-                            const uint64_t *colWidths, uint64_t *root, int family)
+                            const uint64_t *colWidths, uint64_t *root, int family, const IndexedDesc *ix = nullptr)
 {
     if (nCols == 0 || nCols > stream::MAX_COLS || nBitsExt <= nBits || wordsPerRow == 0 || !colWidths || !h_packed ||
         !root)
@@ -1086,13 +1124,21 @@ static int stream_commit_on(uint64_t *slot, uint64_t slot_words, cudaStream_t s,
     const stream::Layout l = stream::layout(nBits, nBitsExt, wordsPerRow);
     if (l.total > slot_words) return set_err(B200_EINVAL, "slot too small for this shape");
     uint64_t tab[2 * stream::MAX_COLS] = {0};
-    if ((rc = stream_tables(tab, colWidths, nCols, wordsPerRow))) return rc;
+    if (ix) {
+        if (!ix->col_source) return set_err(B200_EINVAL, "null column sources");
+        if ((rc = indexed_info(tab, colWidths, nCols, wordsPerRow, *ix))) return rc;
+    } else if ((rc = stream_tables(tab, colWidths, nCols, wordsPerRow))) {
+        return rc;
+    }
     if ((rc = ensure_init_current())) return rc;
     const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
     CK(cudaMemcpyAsync(slot + l.widths, tab, sizeof(tab), cudaMemcpyHostToDevice, s), "tables H2D");
     CK(cudaMemcpyAsync(slot + l.packed, h_packed, N * wordsPerRow * 8, cudaMemcpyHostToDevice, s), "packed H2D");
-    CK(family == 1 ? stream::run<1>(slot, l, nBits, nBitsExt, nCols, wordsPerRow, s)
-                   : stream::run<2>(slot, l, nBits, nBitsExt, nCols, wordsPerRow, s),
+    stream::Indexed sx{};
+    if (ix) sx = stream::Indexed{ix->d_table, ix->num_entries, ix->words_per_entry, ix->index_bits};
+    const stream::Indexed *px = ix ? &sx : nullptr;
+    CK(family == 1 ? stream::run<1>(slot, l, nBits, nBitsExt, nCols, wordsPerRow, s, px)
+                   : stream::run<2>(slot, l, nBits, nBitsExt, nCols, wordsPerRow, s, px),
        "streaming commit");
     const uint64_t tsz = merkle::tree_num_elements(NExt, 4);
     CK(cudaMemcpyAsync(root, slot + l.tree + tsz - 4, 32, cudaMemcpyDeviceToHost, s), "root D2H");
@@ -1166,8 +1212,6 @@ extern "C" int64_t commit_witness_streaming(void *d_buffers, uint64_t slotIdx, u
                                             void *packed, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols,
                                             uint64_t wordsPerRow, void *colWidths, void *root)
 {
-    (void)airgroupId;
-    (void)airId;
     auto *b = (CommitBuffers *)d_buffers;
     if (!b || b->sc_streams.empty()) return -11;
     if (slotIdx >= b->sc_streams.size()) return -12;
@@ -1181,9 +1225,30 @@ extern "C" int64_t commit_witness_streaming(void *d_buffers, uint64_t slotIdx, u
         return -14;
     }
     cudaSetDevice(b->device);
+    IndexedDesc ixd{};
+    const IndexedDesc *ix = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(b->mu);
+        auto it = b->indexed.find({airgroupId, airId});
+        if (it != b->indexed.end()) {
+            if (!it->second.d_table) {
+                b->sc_inflight--;
+                set_err(B200_EINVAL, "indexed air without a registered instruction table");
+                return -16;
+            }
+            if (it->second.col_source.size() != nCols) {
+                b->sc_inflight--;
+                set_err(B200_EINVAL, "indexed air registered with another column count");
+                return -10;
+            }
+            ixd = IndexedDesc{it->second.col_source.data(), it->second.index_bits, it->second.d_table,
+                              it->second.num_entries, it->second.words_per_entry};
+            ix = &ixd;
+        }
+    }
     uint64_t *slot = b->sc_base + slotIdx * (b->sc_slot_bytes / 8);
     int rc = stream_commit_on(slot, b->sc_slot_bytes / 8, b->sc_streams[slotIdx], packed, nBits, nBitsExt, nCols,
-                              wordsPerRow, (const uint64_t *)colWidths, (uint64_t *)root, 1);
+                              wordsPerRow, (const uint64_t *)colWidths, (uint64_t *)root, 1, ix);
     b->sc_inflight--;
     return rc == B200_OK ? 0 : -10;
 }
@@ -1207,4 +1272,107 @@ extern "C" int b200_stream_commit_packed(uint64_t *d_slot, uint64_t slot_words, 
     if (!d_slot) return set_err(B200_EINVAL, "null slot");
     return stream_commit_on(d_slot, slot_words, (cudaStream_t)stream, h_packed, nBits, nBitsExt, nCols, wordsPerRow,
                             colWidths, root, g_native_family.load());
+}
+
+// ------------------------------------------------------------ indexed witness ----
+// Stands in for the setup's PackedInfo of an indexed AIR: which columns come from the
+// instruction table (col_source[c] = 1) and the width of the row's leading index.
+extern "C" int b200_register_indexed_air(void *d_buffers, uint64_t airgroupId, uint64_t airId, uint64_t nCols,
+                                         const uint8_t *col_source, uint64_t index_bits)
+{
+    auto *b = (CommitBuffers *)d_buffers;
+    if (!b || (nCols && !col_source)) return set_err(B200_EINVAL, "null argument");
+    if (index_bits > 64) return set_err(B200_EINVAL, "index header wider than 64 bits");
+    std::lock_guard<std::mutex> lk(b->mu);
+    auto &a = b->indexed[{airgroupId, airId}];
+    a.col_source.assign(col_source, col_source + nCols);
+    a.index_bits = index_bits;
+    return B200_OK;
+}
+
+// register_instruction_table (starks_api.hpp:192): the AIR's instruction table, num_entries
+// entries of words_per_entry words (host), copied to the device and kept with the buffers.
+extern "C" void register_instruction_table(void *d_buffers, uint64_t airgroupId, uint64_t airId, uint64_t *table,
+                                           uint64_t num_entries, uint64_t words_per_entry)
+{
+    auto *b = (CommitBuffers *)d_buffers;
+    if (!b || !table || num_entries == 0) {
+        set_err(B200_EINVAL, "register_instruction_table: empty table");
+        if (b) b->error = B200_EINVAL;
+        return;
+    }
+    std::lock_guard<std::mutex> lk(b->mu);
+    cudaSetDevice(b->device);
+    auto &a = b->indexed[{airgroupId, airId}];
+    if (a.d_table) cudaFree(a.d_table);
+    a.d_table = nullptr;
+    const uint64_t words = num_entries * (words_per_entry ? words_per_entry : 1);
+    if (cudaMalloc((void **)&a.d_table, words * 8) != cudaSuccess ||
+        cudaMemcpy(a.d_table, table, num_entries * words_per_entry * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        if (a.d_table) cudaFree(a.d_table);
+        a.d_table = nullptr;
+        b->error = set_err(B200_ENOMEM, "register_instruction_table: device copy");
+        return;
+    }
+    a.num_entries = num_entries;
+    a.words_per_entry = words_per_entry;
+}
+
+// Native commit of an indexed witness (device rows and table; col_bits, col_source on the host):
+// the reference's unpack_indexed (starks_gpu.cu:125-185) straight into the column-major scratch,
+// then the LDE in place and the tree, like b200_commit_packed_device.
+extern "C" int b200_commit_indexed_device(uint64_t *root_host, uint64_t *d_lde, uint64_t *d_tree,
+                                          const uint64_t *d_rows, uint64_t words_per_row, const uint64_t *d_table,
+                                          uint64_t num_entries, uint64_t words_per_entry, uint64_t index_bits,
+                                          const uint64_t *col_bits, const uint8_t *col_source, uint64_t nBits,
+                                          uint64_t nBitsExt, uint64_t nCols, uint64_t arity, uint64_t *d_scratch,
+                                          void *stream)
+{
+    int rc = check_shape(nBits, nBitsExt, nCols, arity);
+    if (rc) return rc;
+    if (nCols && (!col_bits || !col_source)) return set_err(B200_EINVAL, "null column description");
+    std::vector<uint64_t> info(nCols);
+    const IndexedDesc ix{col_source, index_bits, d_table, num_entries, words_per_entry};
+    if (nCols && (rc = indexed_info(info.data(), col_bits, nCols, words_per_row, ix))) return rc;
+    if ((rc = ensure_init_current())) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
+    if (!d_tree || (nCols && (!d_lde || !d_rows || !d_scratch))) return set_err(B200_EINVAL, "null buffer");
+    if (nCols) {
+        uint64_t *d_info = nullptr;
+        CK(cudaMallocAsync((void **)&d_info, nCols * 8, s), "column info buffer");
+        CK(cudaMemcpyAsync(d_info, info.data(), nCols * 8, cudaMemcpyHostToDevice, s), "column info H2D");
+        {
+            prof::Scope ps(prof::TRANSPOSE, s);
+            unpack::unpack_indexed_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(
+                d_scratch, d_rows, d_table, N, words_per_row, words_per_entry, num_entries, index_bits, d_info, 0,
+                (uint32_t)nCols);
+            prof::count();
+        }
+        const cudaError_t e = cudaGetLastError();
+        cudaFreeAsync(d_info, s);
+        CK(e, "indexed unpack");
+        CK(ntt::lde(d_lde, d_scratch, false, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, d_scratch, s), "lde");
+    }
+    CK(merkle::build_tree_arity(arity, d_tree, d_lde, 1, NExt, nCols, NExt, s, g_native_family.load()), "merkletree");
+    if (root_host) {
+        const uint64_t total = merkle::tree_num_elements(NExt, arity);
+        CK(cudaMemcpyAsync(root_host, d_tree + total - 4, 32, cudaMemcpyDeviceToHost, s), "root D2H");
+        CK(cudaStreamSynchronize(s), "sync");
+    }
+    return B200_OK;
+}
+
+// Native streaming commit of an indexed witness (host rows, device table).
+extern "C" int b200_stream_commit_indexed(uint64_t *d_slot, uint64_t slot_words, const uint64_t *h_rows,
+                                          uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t words_per_row,
+                                          const uint64_t *col_bits, const uint8_t *col_source, uint64_t index_bits,
+                                          const uint64_t *d_table, uint64_t num_entries, uint64_t words_per_entry,
+                                          uint64_t *root, void *stream)
+{
+    if (!d_slot) return set_err(B200_EINVAL, "null slot");
+    const IndexedDesc ix{col_source, index_bits, d_table, num_entries, words_per_entry};
+    return stream_commit_on(d_slot, slot_words, (cudaStream_t)stream, h_rows, nBits, nBitsExt, nCols, words_per_row,
+                            col_bits, root, g_native_family.load(), &ix);
 }

@@ -13,6 +13,7 @@
 #pragma once
 #include "merkle.cuh"
 #include "ntt.cuh"
+#include "unpack.cuh"
 
 namespace stream {
 
@@ -82,21 +83,33 @@ __global__ void __launch_bounds__(merkle::TPB) absorb_kernel(uint64_t *__restric
     for (int i = 0; i < 4; i++) carry[row * 4 + i] = gl::canon(st[i * TPB]);
 }
 
+// Indexed witness: the instruction table on the device and the row header width; the slot's
+// width region then holds width | source << 32 per column (unpack::unpack_indexed_kernel).
+struct Indexed {
+    const uint64_t *table;
+    uint64_t num_entries, words_per_entry, index_bits;
+};
+
 // The whole slot commit on `s` (device work only; the caller copies the packed rows to
 // slot + layout.packed and the widths/offsets to their regions first).  Leaves the tree at
 // slot + layout.tree.
 template <int FAM>
 inline cudaError_t run(uint64_t *slot, const Layout &l, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols,
-                       uint64_t wordsPerRow, cudaStream_t s)
+                       uint64_t wordsPerRow, cudaStream_t s, const Indexed *ix = nullptr)
 {
     const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
     uint64_t *tree = slot + l.tree, *chunk = slot + l.chunk, *scr = slot + l.scratch;
     cudaError_t e;
     for (uint64_t c0 = 0; c0 < nCols; c0 += RATE) {
         const uint32_t cc = (uint32_t)((nCols - c0) < RATE ? (nCols - c0) : RATE);
-        unpack_range_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(scr, slot + l.packed, slot + l.widths,
-                                                                       slot + l.offsets, N, wordsPerRow,
-                                                                       (uint32_t)c0, cc);
+        if (ix)
+            unpack::unpack_indexed_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(
+                scr, slot + l.packed, ix->table, N, wordsPerRow, ix->words_per_entry, ix->num_entries, ix->index_bits,
+                slot + l.widths, (uint32_t)c0, cc);
+        else
+            unpack_range_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(scr, slot + l.packed, slot + l.widths,
+                                                                           slot + l.offsets, N, wordsPerRow,
+                                                                           (uint32_t)c0, cc);
         prof::count();
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         if ((e = ntt::lde(chunk, scr, false, (uint32_t)nBits, (uint32_t)nBitsExt, cc, scr, s)) != cudaSuccess) return e;

@@ -1,4 +1,5 @@
-// Bit-packed witness -> column-major trace, in place of the transpose in front of the LDE.
+// Bit-packed (and indexed) witness -> column-major trace, in place of the transpose in front of
+// the LDE.
 //
 // Packed layout (the reference's PackedInfo / unpack kernel, starks_gpu.cu:49-103): every row
 // is `words_per_row` u64 words; column c occupies the next col_bits[c] bits, least
@@ -42,6 +43,73 @@ __global__ void __launch_bounds__(256) unpack_kernel(uint64_t *__restrict__ dst,
             off = nb - left;
         }
         dst[c * nrows + row] = val;
+    }
+}
+
+// Bit cursor over a packed stream of `words` u64 words: take the next nb (1..64) bits, least
+// significant first, crossing into the next word when needed.  The same walk as unpack_kernel.
+struct Cursor {
+    const uint64_t *base;
+    uint64_t words, word, idx, off;
+    __device__ __forceinline__ void start(const uint64_t *b, uint64_t n)
+    {
+        base = b;
+        words = n;
+        word = n ? __ldg(b) : 0;
+        idx = 0;
+        off = 0;
+    }
+    template <bool EXTRACT>
+    __device__ __forceinline__ uint64_t take(uint64_t nb)
+    {
+        uint64_t val = 0;
+        const uint64_t left = 64 - off;
+        if (nb <= left) {
+            if (EXTRACT) val = (word >> off) & (nb == 64 ? ~0ull : ((1ull << nb) - 1));
+            off += nb;
+            if (off == 64 && idx + 1 < words) {
+                word = __ldg(base + ++idx);
+                off = 0;
+            }
+        } else {
+            const uint64_t low = word >> off;
+            word = __ldg(base + ++idx);
+            if (EXTRACT) val = ((word & ((1ull << (nb - left)) - 1)) << left) | low;
+            off = nb - left;
+        }
+        return val;
+    }
+};
+
+// Indexed witness (the reference's unpack_indexed, starks_gpu.cu:125-185): a row is a leading
+// instruction index (index_bits wide) followed by the runtime columns; the columns flagged in
+// col_info (bit 32) are read instead from entry `index` of a shared instruction table
+// (words_per_entry words per entry, its own bit cursor).  An index past the table selects entry
+// 0, as the reference does.  col_info[c] = width | source << 32.  Columns [c0, c0 + cc) are
+// written (column-major, stride nrows); earlier columns only advance the cursors.
+__global__ void __launch_bounds__(256) unpack_indexed_kernel(uint64_t *__restrict__ dst,
+                                                             const uint64_t *__restrict__ rows,
+                                                             const uint64_t *__restrict__ table, uint64_t nrows,
+                                                             uint64_t words_per_row, uint64_t words_per_entry,
+                                                             uint64_t num_entries, uint64_t index_bits,
+                                                             const uint64_t *__restrict__ col_info, uint32_t c0,
+                                                             uint32_t cc)
+{
+    const uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= nrows) return;
+    Cursor r, t;
+    r.start(rows + row * words_per_row, words_per_row);
+    uint64_t index = index_bits ? r.take<true>(index_bits) : 0;
+    if (index >= num_entries) index = 0;
+    t.start(table + index * words_per_entry, words_per_entry);
+    for (uint32_t c = 0; c < c0 + cc; c++) {
+        const uint64_t info = __ldg(col_info + c), nb = info & 0xffffffffull;
+        Cursor &k = (info >> 32) ? t : r;
+        if (c < c0) {
+            k.take<false>(nb);
+        } else {
+            dst[(uint64_t)(c - c0) * nrows + row] = k.take<true>(nb);
+        }
     }
 }
 
