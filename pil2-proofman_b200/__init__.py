@@ -468,8 +468,10 @@ def pack_indexed(runtime, index, index_bits, table_vals, col_bits, col_source):
     parts.append(runtime)
     widths += rt_bits
     rows = pack_rows(np.concatenate(parts, axis=1), widths) if widths else np.zeros((len(index), 1), np.uint64)
-    table_vals = np.ascontiguousarray(table_vals, dtype=np.uint64).reshape(-1, len(tb_bits))
-    table = pack_rows(table_vals, tb_bits) if tb_bits else np.zeros((table_vals.shape[0], 0), np.uint64)
+    table_vals = np.ascontiguousarray(table_vals, dtype=np.uint64)
+    if not tb_bits:
+        return rows, np.zeros((max(1, table_vals.shape[0] if table_vals.ndim else 1), 0), np.uint64)
+    table = pack_rows(table_vals.reshape(-1, len(tb_bits)), tb_bits)
     return rows, table
 
 
