@@ -338,30 +338,34 @@ __device__ __forceinline__ void radix_phase_fixed(uint64_t *sm)
     }
 }
 
+// Radix of the fixed kernels' phases: 2^NTT_PHASE_BITS points per thread and phase.
+constexpr int NTT_PHASE_BITS = 4;
+
 // DIT: full phases from the low mid bits, then the remainder; DIF: the reverse order
 template <bool DIF, int K, int LGL, int PH>
 __device__ __forceinline__ void phases_fixed(uint64_t *sm)
 {
-    constexpr int FULL = K >> 2, REM = K & 3;
+    constexpr int RP = NTT_PHASE_BITS;
+    constexpr int FULL = K / RP, REM = K % RP;
     if constexpr (!DIF) {
         if constexpr (PH < FULL) {
-            radix_phase_fixed<4, false, K, LGL, 4 * PH>(sm);
+            radix_phase_fixed<RP, false, K, LGL, RP * PH>(sm);
             __syncthreads();
             phases_fixed<false, K, LGL, PH + 1>(sm);
         } else if constexpr (REM != 0) {
-            radix_phase_fixed<REM, false, K, LGL, 4 * FULL>(sm);
+            radix_phase_fixed<REM, false, K, LGL, RP * FULL>(sm);
             __syncthreads();
         }
     } else {
         // PH counts down from FULL (the remainder phase) to 0
         if constexpr (PH == FULL) {
             if constexpr (REM != 0) {
-                radix_phase_fixed<REM, true, K, LGL, 4 * FULL>(sm);
+                radix_phase_fixed<REM, true, K, LGL, RP * FULL>(sm);
                 __syncthreads();
             }
             if constexpr (FULL > 0) phases_fixed<true, K, LGL, FULL - 1>(sm);
         } else {
-            radix_phase_fixed<4, true, K, LGL, 4 * PH>(sm);
+            radix_phase_fixed<RP, true, K, LGL, RP * PH>(sm);
             __syncthreads();
             if constexpr (PH > 0) phases_fixed<true, K, LGL, PH - 1>(sm);
         }
@@ -387,7 +391,7 @@ __global__ void __launch_bounds__(Shape<K, LGL>::NT, 1024 / Shape<K, LGL>::NT) p
     const uint32_t tw_shift = NTT_TWLG - s0 - K;
     const uint32_t rep = a.rep, gshift = a.gshift, goff = (uint32_t)a.goff;
 
-#pragma unroll
+#pragma unroll 4  // full unrolling hoists all 16 loads of a thread and spills at 64 registers
     for (int it = 0; it < IT; it++) {
         const uint32_t q = threadIdx.x + (uint32_t)it * NT;
         if ((T % NT) != 0 && q >= (uint32_t)T) break;
@@ -403,10 +407,10 @@ __global__ void __launch_bounds__(Shape<K, LGL>::NT, 1024 / Shape<K, LGL>::NT) p
     }
     __syncthreads();
     if (inv)
-        phases_fixed<true, K, LGL, (K >> 2)>(sm);
+        phases_fixed<true, K, LGL, K / NTT_PHASE_BITS>(sm);
     else
         phases_fixed<false, K, LGL, 0>(sm);
-#pragma unroll
+#pragma unroll 4  // full unrolling hoists all 16 loads of a thread and spills at 64 registers
     for (int it = 0; it < IT; it++) {
         const uint32_t q = threadIdx.x + (uint32_t)it * NT;
         if ((T % NT) != 0 && q >= (uint32_t)T) break;
