@@ -29,6 +29,10 @@ constexpr int TPB = 128;  // threads per CTA of the hashing kernels (one row / n
 template <int FAM>
 struct Family {
     static constexpr int SMEM_AREAS = FAM == 1 ? 2 : 1;
+    // resident CTAs per SM the register budget must allow (registers <= 64 K / (MIN_CTAS * 128)):
+    // Poseidon1's 32 KB of shared memory per CTA fits 7 CTAs, so its registers are capped to
+    // match (72); Poseidon2 keeps 12 resident CTAs (<= 42 registers, the 40 it needs)
+    static constexpr int MIN_CTAS = FAM == 1 ? 7 : 12;
 };
 
 template <int W, int FAM>
@@ -72,7 +76,7 @@ __device__ __forceinline__ void leaf_row(uint64_t *st, uint64_t *__restrict__ di
 }
 
 template <int W, int FAM = 2>
-__global__ void __launch_bounds__(TPB) leaf_hash_kernel(uint64_t *__restrict__ digests,
+__global__ void __launch_bounds__(TPB, Family<FAM>::MIN_CTAS) leaf_hash_kernel(uint64_t *__restrict__ digests,
                                                         const uint64_t *__restrict__ src, uint64_t rs,
                                                         uint64_t cs, uint64_t ncols, uint64_t nrows)
 {
@@ -113,7 +117,7 @@ __device__ __forceinline__ void node_one(uint64_t *st, uint64_t *__restrict__ le
 }
 
 template <int W, int FAM = 2>
-__global__ void __launch_bounds__(TPB) node_kernel(uint64_t *__restrict__ level, uint64_t pending, uint64_t pad,
+__global__ void __launch_bounds__(TPB, Family<FAM>::MIN_CTAS) node_kernel(uint64_t *__restrict__ level, uint64_t pending, uint64_t pad,
                                                    uint64_t parents, uint64_t *__restrict__ out)
 {
     __shared__ uint64_t sm[Family<FAM>::SMEM_AREAS * W * TPB];
@@ -123,7 +127,7 @@ __global__ void __launch_bounds__(TPB) node_kernel(uint64_t *__restrict__ level,
 
 // Whole permutations of n independent states (permute / permuteTrunc checks).
 template <int W, int FAM = 2>
-__global__ void __launch_bounds__(TPB) permute_kernel(uint64_t *__restrict__ out, const uint64_t *__restrict__ in,
+__global__ void __launch_bounds__(TPB, Family<FAM>::MIN_CTAS) permute_kernel(uint64_t *__restrict__ out, const uint64_t *__restrict__ in,
                                                       uint64_t n)
 {
     __shared__ uint64_t sm[Family<FAM>::SMEM_AREAS * W * TPB];

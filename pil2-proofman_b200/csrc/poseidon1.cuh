@@ -151,7 +151,10 @@ __device__ __forceinline__ void sbox_add(uint64_t *st, const uint64_t *c)
 }
 
 // The permutation of the thread's state st[i*TPB] (loose words in, loose words out);
-// tmp: a second W x TPB area of the thread.
+// tmp: a second W x TPB area of the thread.  The eight full rounds run as one loop (round 3
+// applies P instead of M, the partial rounds sit between rounds 3 and 4, the last round adds no
+// constants) so the S-box and matrix code appears once: unrolled copies overflowed the
+// instruction cache.
 template <int W, int TPB>
 __device__ __forceinline__ void permute_smem(uint64_t *st, uint64_t *tmp)
 {
@@ -160,35 +163,32 @@ __device__ __forceinline__ void permute_smem(uint64_t *st, uint64_t *tmp)
 #pragma unroll
     for (int i = 0; i < W; i++) st[i * TPB] = gl::add_c(st[i * TPB], C[i]);
 #pragma unroll 1
-    for (int r = 0; r < 3; r++) {
-        sbox_add<W, TPB>(st, C + (r + 1) * W);
-        mvp_small<W, TPB>(st, tmp);
-    }
-    sbox_add<W, TPB>(st, C + 4 * W);
-    mvp_full<W, TPB>(st, tmp, Tab<W>::P());
-    uint64_t x0 = st[0];
+    for (int r = 0; r < 8; r++) {
+        if (r == 4) {
+            uint64_t x0 = st[0];
 #pragma unroll 1
-    for (int r = 0; r < NPARTIAL; r++) {
-        const uint64_t *Sr = S + (2 * W - 1) * r;
-        x0 = gl::add_c(gl::pow7(x0), C[5 * W + r]);
-        Acc160 a = {{0, 0, 0, 0, 0}};
-        acc160_mul_add(a, x0, Sr[0]);
+            for (int pr = 0; pr < NPARTIAL; pr++) {
+                const uint64_t *Sr = S + (2 * W - 1) * pr;
+                x0 = gl::add_c(gl::pow7(x0), C[5 * W + pr]);
+                Acc160 a = {{0, 0, 0, 0, 0}};
+                acc160_mul_add(a, x0, Sr[0]);
 #pragma unroll 4
-        for (int i = 1; i < W; i++) {
-            const uint64_t xi = st[i * TPB];
-            acc160_mul_add(a, xi, Sr[i]);
-            st[i * TPB] = gl::mul_add(x0, Sr[W - 1 + i], xi);
+                for (int i = 1; i < W; i++) {
+                    const uint64_t xi = st[i * TPB];
+                    acc160_mul_add(a, xi, Sr[i]);
+                    st[i * TPB] = gl::mul_add(x0, Sr[W - 1 + i], xi);
+                }
+                x0 = acc160_reduce(a);
+            }
+            st[0] = x0;
         }
-        x0 = acc160_reduce(a);
+        const uint64_t *c = r < 4 ? C + (r + 1) * W : (r < 7 ? C + 5 * W + NPARTIAL + (r - 4) * W : nullptr);
+        sbox_add<W, TPB>(st, c);
+        if (r == 3)
+            mvp_full<W, TPB>(st, tmp, Tab<W>::P());
+        else
+            mvp_small<W, TPB>(st, tmp);
     }
-    st[0] = x0;
-#pragma unroll 1
-    for (int r = 0; r < 3; r++) {
-        sbox_add<W, TPB>(st, C + 5 * W + NPARTIAL + r * W);
-        mvp_small<W, TPB>(st, tmp);
-    }
-    sbox_add<W, TPB>(st, nullptr);
-    mvp_small<W, TPB>(st, tmp);
 }
 
 }  // namespace p1

@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(256) unpack_range_kernel(uint64_t *__restrict_
 // Absorb one chunk of cc <= RATE extended columns (column-major, stride nrows) into the carried
 // words `carry` (row-major, 4 per row = tree level 0).
 template <int FAM>
-__global__ void __launch_bounds__(merkle::TPB) absorb_kernel(uint64_t *__restrict__ carry,
+__global__ void __launch_bounds__(merkle::TPB, merkle::Family<FAM>::MIN_CTAS) absorb_kernel(uint64_t *__restrict__ carry,
                                                              const uint64_t *__restrict__ chunk, uint32_t cc,
                                                              int first, uint64_t nrows)
 {
