@@ -83,6 +83,63 @@ __global__ void __launch_bounds__(512, 2) pass_grouped(const PassEntry *e, int n
     ntt::pass16_body(p, local % tiles, local / tiles);
 }
 
+// Grouped fixed-shape window: every entry of the launch has window shape (K, LGL).
+template <int K, int LGL>
+__global__ void __launch_bounds__(ntt::Shape<K, LGL>::NT, 1024 / ntt::Shape<K, LGL>::NT)
+    pass_fixed_grouped(const PassEntry *e, int n)
+{
+    const int i = find_entry(e, n, blockIdx.x);
+    const uint64_t local = blockIdx.x - e[i].begin;
+    const uint64_t tiles = e[i].tiles;
+    const ntt::Pass p = e[i].p;
+    ntt::pass_fixed_body<K, LGL>(p, (uint32_t)(local % tiles), local / tiles);
+}
+
+typedef void (*GroupedKernel)(const PassEntry *, int);
+
+template <int K>
+inline GroupedKernel grouped_fixed_k(uint32_t lgL)
+{
+    if (lgL == 13 - K) return pass_fixed_grouped<K, 13 - K>;
+    if (lgL == 0) return pass_fixed_grouped<K, 0>;
+    return nullptr;
+}
+
+// the grouped fixed-shape kernel of a window shape, or null (the generic grouped kernel serves it)
+inline GroupedKernel grouped_fixed(uint32_t k, uint32_t lgL)
+{
+    switch (k) {
+    case 1: return grouped_fixed_k<1>(lgL);
+    case 2: return grouped_fixed_k<2>(lgL);
+    case 3: return grouped_fixed_k<3>(lgL);
+    case 4: return grouped_fixed_k<4>(lgL);
+    case 5: return grouped_fixed_k<5>(lgL);
+    case 6: return grouped_fixed_k<6>(lgL);
+    case 7: return grouped_fixed_k<7>(lgL);
+    case 8: return grouped_fixed_k<8>(lgL);
+    case 9: return grouped_fixed_k<9>(lgL);
+    case 10: return grouped_fixed_k<10>(lgL);
+    case 11: return grouped_fixed_k<11>(lgL);
+    case 12: return grouped_fixed_k<12>(lgL);
+    default: return nullptr;
+    }
+}
+
+inline cudaError_t set_grouped_fixed_attrs()
+{
+    for (uint32_t k = 1; k <= NTT_KMAX; k++) {
+        const uint32_t shapes[2] = {13 - k, 0};
+        for (uint32_t lgL : shapes) {
+            GroupedKernel g = grouped_fixed(k, lgL);
+            if (!g) continue;
+            const uint32_t T = 1u << (k + lgL);
+            cudaError_t e = cudaFuncSetAttribute(g, cudaFuncAttributeMaxDynamicSharedMemorySize, (T + T / 16) * 8);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
+}
+
 // Persistent leaf sponge: CTAs claim 128-row blocks from *counter until `total` is reached.
 template <int W>
 __global__ void __launch_bounds__(merkle::TPB) leaf_persistent(const LeafEntry *e, int n, uint64_t total,
@@ -122,12 +179,13 @@ __global__ void gather_roots(const uint64_t *const *tree_ends, int n, uint64_t *
 // ------------------------------------------------------------------ host plan ----
 
 struct Launch {
-    int kind;  // 0 transpose, 1 pass, 2 leaf, 3 node, 4 roots
+    int kind;  // 0 transpose, 1 pass (generic), 2 leaf, 3 node, 5 pass (fixed shape width, lgl)
     int width;
     size_t off;  // byte offset of the entry array in the device table buffer
     int n;
     uint64_t blocks;
     size_t smem;
+    int lgl = 0;
 };
 
 class Plan {
@@ -152,6 +210,44 @@ class Plan {
         graph = nullptr;
         d_table = nullptr;
         h_roots = nullptr;
+    }
+
+    // one window index's entries as launches: one per fixed window shape, the rest generic
+    void push_passes(const std::vector<PassEntry> &pe)
+    {
+        std::vector<std::pair<uint32_t, uint32_t>> shapes;
+        for (const PassEntry &e : pe) {
+            const std::pair<uint32_t, uint32_t> sh{e.p.k, e.p.lgL};
+            if (grouped_fixed(sh.first, sh.second) &&
+                std::find(shapes.begin(), shapes.end(), sh) == shapes.end())
+                shapes.push_back(sh);
+        }
+        for (const auto &sh : shapes) {
+            std::vector<PassEntry> g;
+            uint64_t b = 0;
+            for (PassEntry e : pe)
+                if (e.p.k == sh.first && e.p.lgL == sh.second) {
+                    e.begin = b;
+                    b += e.tiles * e.ncols;
+                    g.push_back(e);
+                }
+            const size_t T = 1ull << (sh.first + sh.second);
+            Launch L{5, (int)sh.first, push(g), (int)g.size(), b, (T + T / 16) * 8};
+            L.lgl = (int)sh.second;
+            launches.push_back(L);
+        }
+        std::vector<PassEntry> rest;
+        uint64_t b = 0;
+        size_t smem = 0;
+        for (PassEntry e : pe)
+            if (!grouped_fixed(e.p.k, e.p.lgL)) {
+                e.begin = b;
+                b += e.tiles * e.ncols;
+                const size_t T = 1ull << (e.p.k + e.p.lgL);
+                smem = std::max(smem, (T + T / 16) * 8);
+                rest.push_back(e);
+            }
+        if (!rest.empty()) launches.push_back(Launch{1, 0, push(rest), (int)rest.size(), b, smem});
     }
 
     template <typename T>
@@ -228,7 +324,8 @@ class Plan {
                 smem = std::max(smem, (T + T / 16) * 8);
                 pe.push_back(e);
             }
-            if (!pe.empty()) launches.push_back(Launch{1, 0, push(pe), (int)pe.size(), b, smem});
+            (void)smem;
+            if (!pe.empty()) push_passes(pe);
         }
         for (int j = 0; j < maxf; j++) {
             std::vector<PassEntry> pe;
@@ -260,7 +357,8 @@ class Plan {
                 smem = std::max(smem, (T + T / 16) * 8);
                 pe.push_back(e);
             }
-            if (!pe.empty()) launches.push_back(Launch{1, 0, push(pe), (int)pe.size(), b, smem});
+            (void)smem;
+            if (!pe.empty()) push_passes(pe);
         }
         // leaves (one persistent launch per arity) and tree levels
         n_counters = 0;
@@ -338,6 +436,13 @@ class Plan {
             switch (L.kind) {
             case 0: transpose_grouped<<<(unsigned)L.blocks, dim3(32, 8), 0, s>>>((const TransposeEntry *)ent, L.n); break;
             case 1: pass_grouped<<<(unsigned)L.blocks, 512, L.smem, s>>>((const PassEntry *)ent, L.n); break;
+            case 5: {
+                const uint32_t T = 1u << (L.width + L.lgl);
+                const uint32_t nt = T / 16 < 32 ? 32 : T / 16 > 512 ? 512 : T / 16;
+                grouped_fixed((uint32_t)L.width, (uint32_t)L.lgl)<<<(unsigned)L.blocks, nt, L.smem, s>>>(
+                    (const PassEntry *)ent, L.n);
+                break;
+            }
             case 2: {
                 const unsigned ctas = (unsigned)std::min<uint64_t>(L.blocks, (uint64_t)leaf_ctas);
                 const LeafEntry *le = (const LeafEntry *)ent;

@@ -27,6 +27,7 @@ static int batch_kernel_attrs()
         CK(cudaFuncSetAttribute(batch::pass_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (NTT_TILE_MAX + NTT_TILE_MAX / 16) * 8),
            "pass_grouped smem attribute");
+        CK(batch::set_grouped_fixed_attrs(), "pass_fixed_grouped smem attributes");
         done[dev] = true;
     }
     return B200_OK;

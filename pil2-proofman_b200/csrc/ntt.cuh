@@ -372,15 +372,14 @@ __device__ __forceinline__ void phases_fixed(uint64_t *sm)
     }
 }
 
+// One CTA of Shape<K,LGL>::NT threads: tile `tile` of column `col` of the window `a`.
 template <int K, int LGL>
-__global__ void __launch_bounds__(Shape<K, LGL>::NT, 1024 / Shape<K, LGL>::NT) pass_fixed_kernel(Pass a)
+__device__ __forceinline__ void pass_fixed_body(const Pass &a, uint32_t tile, uint64_t col)
 {
     extern __shared__ uint64_t sm[];
     constexpr int T = Shape<K, LGL>::T, NT = Shape<K, LGL>::NT;
     constexpr int IT = (T + NT - 1) / NT;
     constexpr uint32_t Lm = (1u << LGL) - 1;
-    const uint32_t tile = blockIdx.x;
-    const uint64_t col = blockIdx.y;
     const uint32_t s0 = a.s0;
     const uint32_t nlob = s0 - LGL;
     const uint32_t hi = tile >> nlob, lob = tile & ((1u << nlob) - 1);
@@ -430,6 +429,12 @@ __global__ void __launch_bounds__(Shape<K, LGL>::NT, 1024 / Shape<K, LGL>::NT) p
         }
         D[pos] = v;
     }
+}
+
+template <int K, int LGL>
+__global__ void __launch_bounds__(Shape<K, LGL>::NT, 1024 / Shape<K, LGL>::NT) pass_fixed_kernel(Pass a)
+{
+    pass_fixed_body<K, LGL>(a, blockIdx.x, blockIdx.y);
 }
 
 typedef void (*PassKernel)(Pass);

@@ -279,7 +279,7 @@ extern "C" const char *b200_kernel_names(void)
     return "pass16_kernel\ntranspose_kernel\nleaf_hash_kernel\nnode_kernel\npermute_kernel\nlde_rows_kernel\n"
            "fill_kernel\nimad_probe_kernel\ntranspose_grouped\npass_grouped\nleaf_persistent\n"
            "node_grouped\ngather_roots\npass_fixed_kernel\nopenings_kernel\nunpack_kernel\nunpack_indexed_kernel\n"
-           "unpack_range_kernel\nabsorb_kernel\n";
+           "unpack_range_kernel\nabsorb_kernel\npass_fixed_grouped\n";
 }
 
 // ------------------------------------------------------------ host-buffer API ----
