@@ -150,8 +150,8 @@ uint64_t b200_tree_num_elements(uint64_t nrows, uint64_t arity);
 /* Hash family of the native b200_* entry points: 1 = Poseidon1 (PoseidonGoldilocks<W>),
  * 2 = Poseidon2 (default), the values of set_hash_family (starks_api.hpp:28).  The reference
  * entry points follow set_hash_family, which may be set once per process; the native ones may
- * switch at any time (not while a call is running).  The batched plan and the commit server
- * support family 2 only (B200_EFAMILY otherwise). */
+ * switch at any time (not while a call is running); a batched plan and a commit server keep
+ * the family they were created under. */
 int b200_set_native_hash_family(int family);
 int b200_native_hash_family(void);
 /* words of scratch the LDE needs (one column-major copy of the trace) */

@@ -141,11 +141,11 @@ inline cudaError_t set_grouped_fixed_attrs()
 }
 
 // Persistent leaf sponge: CTAs claim 128-row blocks from *counter until `total` is reached.
-template <int W>
-__global__ void __launch_bounds__(merkle::TPB) leaf_persistent(const LeafEntry *e, int n, uint64_t total,
-                                                              unsigned long long *counter)
+template <int W, int FAM>
+__global__ void __launch_bounds__(merkle::TPB, merkle::Family<FAM>::MIN_CTAS)
+    leaf_persistent(const LeafEntry *e, int n, uint64_t total, unsigned long long *counter)
 {
-    __shared__ uint64_t sm[W * merkle::TPB];
+    __shared__ uint64_t sm[merkle::Family<FAM>::SMEM_AREAS * W * merkle::TPB];
     __shared__ uint64_t claim;
     for (;;) {
         if (threadIdx.x == 0) claim = atomicAdd(counter, 1ull);
@@ -156,18 +156,18 @@ __global__ void __launch_bounds__(merkle::TPB) leaf_persistent(const LeafEntry *
         const int i = find_entry(e, n, b);
         const LeafEntry L = e[i];
         const uint64_t row = (b - L.begin) * merkle::TPB + threadIdx.x;
-        if (row < L.nrows) merkle::leaf_row<W>(sm + threadIdx.x, L.digests, L.src, 1, L.nrows, L.ncols, row);
+        if (row < L.nrows) merkle::leaf_row<W, FAM>(sm + threadIdx.x, L.digests, L.src, 1, L.nrows, L.ncols, row);
     }
 }
 
-template <int W>
-__global__ void __launch_bounds__(merkle::TPB) node_grouped(const NodeEntry *e, int n)
+template <int W, int FAM>
+__global__ void __launch_bounds__(merkle::TPB, merkle::Family<FAM>::MIN_CTAS) node_grouped(const NodeEntry *e, int n)
 {
-    __shared__ uint64_t sm[W * merkle::TPB];
+    __shared__ uint64_t sm[merkle::Family<FAM>::SMEM_AREAS * W * merkle::TPB];
     const int i = find_entry(e, n, blockIdx.x);
     const NodeEntry E = e[i];
     const uint64_t idx = (blockIdx.x - E.begin) * merkle::TPB + threadIdx.x;
-    if (idx < E.parents) merkle::node_one<W>(sm + threadIdx.x, E.level, E.pending, E.pad, E.parents, E.out, idx);
+    if (idx < E.parents) merkle::node_one<W, FAM>(sm + threadIdx.x, E.level, E.pending, E.pad, E.parents, E.out, idx);
 }
 
 __global__ void gather_roots(const uint64_t *const *tree_ends, int n, uint64_t *roots)
@@ -199,6 +199,7 @@ class Plan {
     uint64_t *h_roots = nullptr;  // pinned, 4 words per instance
     cudaGraphExec_t graph = nullptr;
     int leaf_ctas = 0;
+    int family = 2;  // hash family of the leaves and levels (1 = Poseidon1, 2 = Poseidon2)
 
     ~Plan() { release(); }
 
@@ -260,9 +261,10 @@ class Plan {
     }
 
     // Builds the launch list for `in`; returns false on an unsupported shape.
-    bool build(const std::vector<Inst> &in, int sm_count)
+    bool build(const std::vector<Inst> &in, int sm_count, int fam = 2)
     {
         inst = in;
+        family = fam == 1 ? 1 : 2;
         launches.clear();
         table.clear();
         // transpose
@@ -410,7 +412,8 @@ class Plan {
         roots_off = push(zeros);
         std::vector<unsigned long long> ctr(n_counters ? n_counters : 1, 0ull);
         counters_off = push(ctr);
-        leaf_ctas = sm_count * 12;
+        leaf_ctas = sm_count * merkle::Family<2>::MIN_CTAS;
+        if (family == 1) leaf_ctas = sm_count * merkle::Family<1>::MIN_CTAS;
         return true;
     }
 
@@ -446,16 +449,28 @@ class Plan {
             case 2: {
                 const unsigned ctas = (unsigned)std::min<uint64_t>(L.blocks, (uint64_t)leaf_ctas);
                 const LeafEntry *le = (const LeafEntry *)ent;
-                if (L.width == 8) leaf_persistent<8><<<ctas, merkle::TPB, 0, s>>>(le, L.n, L.blocks, ctr + L.smem);
-                if (L.width == 12) leaf_persistent<12><<<ctas, merkle::TPB, 0, s>>>(le, L.n, L.blocks, ctr + L.smem);
-                if (L.width == 16) leaf_persistent<16><<<ctas, merkle::TPB, 0, s>>>(le, L.n, L.blocks, ctr + L.smem);
+                if (family == 1) {
+                    if (L.width == 8) leaf_persistent<8, 1><<<ctas, merkle::TPB, 0, s>>>(le, L.n, L.blocks, ctr + L.smem);
+                    if (L.width == 12) leaf_persistent<12, 1><<<ctas, merkle::TPB, 0, s>>>(le, L.n, L.blocks, ctr + L.smem);
+                    if (L.width == 16) leaf_persistent<16, 1><<<ctas, merkle::TPB, 0, s>>>(le, L.n, L.blocks, ctr + L.smem);
+                } else {
+                    if (L.width == 8) leaf_persistent<8, 2><<<ctas, merkle::TPB, 0, s>>>(le, L.n, L.blocks, ctr + L.smem);
+                    if (L.width == 12) leaf_persistent<12, 2><<<ctas, merkle::TPB, 0, s>>>(le, L.n, L.blocks, ctr + L.smem);
+                    if (L.width == 16) leaf_persistent<16, 2><<<ctas, merkle::TPB, 0, s>>>(le, L.n, L.blocks, ctr + L.smem);
+                }
                 break;
             }
             case 3: {
                 const NodeEntry *ne = (const NodeEntry *)ent;
-                if (L.width == 8) node_grouped<8><<<(unsigned)L.blocks, merkle::TPB, 0, s>>>(ne, L.n);
-                if (L.width == 12) node_grouped<12><<<(unsigned)L.blocks, merkle::TPB, 0, s>>>(ne, L.n);
-                if (L.width == 16) node_grouped<16><<<(unsigned)L.blocks, merkle::TPB, 0, s>>>(ne, L.n);
+                if (family == 1) {
+                    if (L.width == 8) node_grouped<8, 1><<<(unsigned)L.blocks, merkle::TPB, 0, s>>>(ne, L.n);
+                    if (L.width == 12) node_grouped<12, 1><<<(unsigned)L.blocks, merkle::TPB, 0, s>>>(ne, L.n);
+                    if (L.width == 16) node_grouped<16, 1><<<(unsigned)L.blocks, merkle::TPB, 0, s>>>(ne, L.n);
+                } else {
+                    if (L.width == 8) node_grouped<8, 2><<<(unsigned)L.blocks, merkle::TPB, 0, s>>>(ne, L.n);
+                    if (L.width == 12) node_grouped<12, 2><<<(unsigned)L.blocks, merkle::TPB, 0, s>>>(ne, L.n);
+                    if (L.width == 16) node_grouped<16, 2><<<(unsigned)L.blocks, merkle::TPB, 0, s>>>(ne, L.n);
+                }
                 break;
             }
             }

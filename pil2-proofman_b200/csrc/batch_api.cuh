@@ -39,10 +39,6 @@ extern "C" void *b200_batch_plan_new(const B200BatchInstance *inst, uint64_t n)
         set_err(B200_EINVAL, "b200_batch_plan_new: empty batch");
         return nullptr;
     }
-    if (g_native_family.load() != 2) {
-        set_err(B200_EFAMILY, "the batched plan hashes with Poseidon2 only");
-        return nullptr;
-    }
     if (ensure_init_current() || batch_kernel_attrs()) return nullptr;
     std::vector<batch::Inst> v;
     if (batch_insts(inst, n, v)) return nullptr;
@@ -50,7 +46,7 @@ extern "C" void *b200_batch_plan_new(const B200BatchInstance *inst, uint64_t n)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     auto *plan = new batch::Plan();
-    if (!plan->build(v, sms)) {
+    if (!plan->build(v, sms, g_native_family.load())) {
         delete plan;
         set_err(B200_EINVAL, "b200_batch_plan_new: unsupported shape");
         return nullptr;

@@ -55,6 +55,7 @@ class Server {
     std::thread worker;
     cudaMemPool_t pool = nullptr;
     cudaEvent_t last_done = nullptr;  // completion event of the most recently admitted request
+    int family = 2;                   // hash family of this server's commits (fixed at creation)
 
     int start(int dev, uint64_t budget_bytes, uint32_t slots)
     {
@@ -187,7 +188,7 @@ class Server {
         // request's kernels); interleaved requests would each take longer and finish together
         if (!rc && last_done) cudaStreamWaitEvent(s, last_done, 0);
         if (!rc) rc = commit_device_fam(nullptr, r->d_lde, r->d_tree, r->d_trace, 1, r->nBits, r->nBitsExt, r->nCols,
-                                        r->arity, r->d_scratch, s, 2);
+                                        r->arity, r->d_scratch, s, family);
         if (!rc && cudaMemcpyAsync(r->h_root, r->d_tree + r->words_tree - 4, 32, cudaMemcpyDeviceToHost, s) !=
                        cudaSuccess)
             rc = B200_ECUDA;
@@ -296,11 +297,9 @@ extern "C" void *b200_server_new(int device, uint64_t budget_bytes, uint32_t slo
         set_err(B200_EINVAL, "slots must be 1..64");
         return nullptr;
     }
-    if (g_native_family.load() != 2) {
-        set_err(B200_EFAMILY, "the commit server hashes with Poseidon2 only");
-        return nullptr;
-    }
+
     auto *s = new serve::Server();
+    s->family = g_native_family.load();
     if (s->start(device, budget_bytes, slots)) {
         delete s;
         return nullptr;

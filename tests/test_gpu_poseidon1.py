@@ -131,11 +131,39 @@ def test_p1_queries_hash_to_root(p1dev, torch_cuda, orc1):
         assert (orc1.root_from_proof(out[i], nc, 1 << nbe, ar, int(r)) == root).all()
 
 
-def test_p1_batch_and_server_refuse(p1dev, torch_cuda):
+def test_p1_batch_and_server(p1dev, torch_cuda, orc1):
+    """The batched plan and the commit server hash with the family they were created under."""
+    torch = torch_cuda
     lib = p1dev.load()
-    assert not lib.b200_server_new(0, 1 << 30, 2)
-    descs = (p1dev.BatchInstance * 1)()
-    assert not lib.b200_batch_plan_new(descs, 1)
+    shapes = [(8, 9, 13), (10, 11, 5), (9, 11, 30), (6, 7, 1)]
+    traces = [oracle.random_field((1 << nb, nc), 500 + i) for i, (nb, nbe, nc) in enumerate(shapes)]
+    exp = [orc1.commit(t, nbe, 4)[0] for t, (nb, nbe, nc) in zip(traces, shapes)]
+    keep = []
+    descs = (p1dev.BatchInstance * len(shapes))()
+    for i, ((nb, nbe, nc), t) in enumerate(zip(shapes, traces)):
+        bufs = [to_dev(torch, t), torch.zeros((1 << nb) * nc, dtype=torch.int64, device="cuda"),
+                torch.zeros((1 << nbe) * nc, dtype=torch.int64, device="cuda"),
+                torch.zeros(p1dev.tree_num_elements(1 << nbe, 4), dtype=torch.int64, device="cuda")]
+        keep.append(bufs)
+        d = descs[i]
+        d.d_trace, d.d_scratch, d.d_lde, d.d_tree = [b.data_ptr() for b in bufs]
+        d.nBits, d.nBitsExt, d.nCols, d.arity = nb, nbe, nc, 4
+    roots = np.zeros((len(shapes), 4), dtype=np.uint64)
+    assert lib.b200_commit_batch_device(descs, len(shapes), roots.ctypes.data, None) == 0, lib.b200_last_error()
+    for i in range(len(shapes)):
+        assert (roots[i] == exp[i]).all(), i
+    srv = lib.b200_server_new(0, 1 << 30, 2)
+    assert srv
+    try:
+        outs = [np.zeros(4, dtype=np.uint64) for _ in shapes]
+        ids = [lib.b200_server_submit(srv, t.ctypes.data, nb, nbe, nc, 4, o.ctypes.data)
+               for t, (nb, nbe, nc), o in zip(traces, shapes, outs)]
+        assert all(i > 0 for i in ids)
+        assert lib.b200_server_wait_all(srv, 60000) == 0
+        for o, e in zip(outs, exp):
+            assert (o == e).all()
+    finally:
+        lib.b200_server_free(srv)
 
 
 _CHILD = r"""
