@@ -390,19 +390,36 @@ __device__ __forceinline__ void pass_fixed_body(const Pass &a, uint32_t tile, ui
     const uint32_t tw_shift = NTT_TWLG - s0 - K;
     const uint32_t rep = a.rep, gshift = a.gshift, goff = (uint32_t)a.goff;
 
-#pragma unroll 4  // full unrolling hoists all 16 loads of a thread and spills at 64 registers
-    for (int it = 0; it < IT; it++) {
-        const uint32_t q = threadIdx.x + (uint32_t)it * NT;
-        if ((T % NT) != 0 && q >= (uint32_t)T) break;
-        const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
-        uint64_t v = S[((pos >> rep) << gshift) + goff];
-        if (a.scale) v = gl::mul(v, a.scale);
-        if (!inv && s0 > 0) {
-            const uint32_t lo = (lob << LGL) | (q & Lm);
-            const uint32_t E = (__brev(q >> LGL) >> (32 - K)) * lo;
-            if (E) v = gl::mul(v, big_twiddle((uint64_t)(E << tw_shift), false));
+    if (inv && rep == 0 && gshift == 0 && goff == 0 && a.scale == 0) {
+        // Inverse (DIF) windows load a plain gather: every element of the tile goes straight to
+        // shared memory with cp.async (no registers, all of a thread's copies in flight at once).
+        // The forward windows keep the register path: their load-time twiddle as a separate
+        // shared-memory pass measured slower.
+#pragma unroll
+        for (int it = 0; it < IT; it++) {
+            const uint32_t q = threadIdx.x + (uint32_t)it * NT;
+            if ((T % NT) != 0 && q >= (uint32_t)T) break;
+            const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
+            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(sm + pad16(q));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(S + pos) : "memory");
         }
-        sm[pad16(q)] = v;
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    } else {
+#pragma unroll 4  // full unrolling hoists all 16 loads of a thread and spills at 64 registers
+        for (int it = 0; it < IT; it++) {
+            const uint32_t q = threadIdx.x + (uint32_t)it * NT;
+            if ((T % NT) != 0 && q >= (uint32_t)T) break;
+            const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
+            uint64_t v = S[((pos >> rep) << gshift) + goff];
+            if (a.scale) v = gl::mul(v, a.scale);
+            if (!inv && s0 > 0) {
+                const uint32_t lo = (lob << LGL) | (q & Lm);
+                const uint32_t E = (__brev(q >> LGL) >> (32 - K)) * lo;
+                if (E) v = gl::mul(v, big_twiddle((uint64_t)(E << tw_shift), false));
+            }
+            sm[pad16(q)] = v;
+        }
     }
     __syncthreads();
     if (inv)
