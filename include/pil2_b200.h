@@ -357,6 +357,16 @@ int b200_stream_commit_indexed(uint64_t *d_slot, uint64_t slot_words, const uint
                                const uint8_t *col_source, uint64_t index_bits, const uint64_t *d_table,
                                uint64_t num_entries, uint64_t words_per_entry, uint64_t *root, void *stream);
 
+/* MerkleTreeGL::getLevel (merkleTreeGL.cpp:84-101): the first level of <= arity^llv nodes, zero-filled
+ * to arity^llv nodes (b200_tree_last_level_words words) — what llv-deep openings are checked against. */
+uint64_t b200_tree_last_level_words(uint64_t arity, uint64_t last_level_verification);
+int b200_tree_last_level_device(uint64_t *d_out, const uint64_t *d_tree, uint64_t NExt, uint64_t arity,
+                                uint64_t last_level_verification, void *stream);
+/* merkletreeReduce (Poseidon2Goldilocks<W>::merkletreeReduce, W = 4 * arity; native hash family):
+ * the tree above n digests (4 words each) in d_tree (b200_tree_num_elements(n, arity) words). */
+int b200_merkletree_reduce_device(uint64_t *root_host, const uint64_t *d_digests, uint64_t n, uint64_t arity,
+                                  uint64_t *d_tree, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -105,6 +105,9 @@ _SIGS = {
     "commit_witness_streaming": (ctypes.c_int64, [_vp, _u64, _u64, _u64, _vp, _u64, _u64, _u64, _u64, _vp, _vp]),
     "stream_commit_pause": (None, []),
     "b200_stream_commit_packed": (_i32, [_vp, _u64, _vp, _u64, _u64, _u64, _u64, _vp, _vp, _vp]),
+    "b200_tree_last_level_words": (_u64, [_u64, _u64]),
+    "b200_tree_last_level_device": (_i32, [_vp, _vp, _u64, _u64, _u64, _vp]),
+    "b200_merkletree_reduce_device": (_i32, [_vp, _vp, _u64, _u64, _vp, _vp]),
     # indexed witness
     "register_instruction_table": (None, [_vp, _u64, _u64, _vp, _u64, _u64]),
     "b200_register_indexed_air": (_i32, [_vp, _u64, _u64, _u64, _vp, _u64]),
@@ -497,4 +500,16 @@ def stream_commit_indexed(d_slot, slot_words, rows, col_bits, col_source, index_
                                              rows.shape[1], bits.ctypes.data, srcs.ctypes.data, index_bits,
                                              _ptr(d_table), num_entries, words_per_entry, root.ctypes.data,
                                              _stream(stream)))
+    return root
+
+
+# ---------------------------------------------------------------- tree level, digest reduction ----
+def tree_last_level_device(d_out, d_tree, next_, arity, llv, stream=None):
+    _check(load().b200_tree_last_level_device(_ptr(d_out), _ptr(d_tree), next_, arity, llv, _stream(stream)))
+
+
+def merkletree_reduce_device(d_digests, n, arity, d_tree, stream=None):
+    root = np.zeros(4, dtype=np.uint64)
+    _check(load().b200_merkletree_reduce_device(root.ctypes.data, _ptr(d_digests), n, arity, _ptr(d_tree),
+                                                _stream(stream)))
     return root

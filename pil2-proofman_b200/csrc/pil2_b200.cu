@@ -1376,3 +1376,60 @@ extern "C" int b200_stream_commit_indexed(uint64_t *d_slot, uint64_t slot_words,
     return stream_commit_on(d_slot, slot_words, (cudaStream_t)stream, h_rows, nBits, nBitsExt, nCols, words_per_row,
                             col_bits, root, g_native_family.load(), &ix);
 }
+
+// ------------------------------------------------ tree level and digest reduction ----
+// MerkleTreeGL::getLevel (merkleTreeGL.cpp:84-101): with last_level_verification = llv > 0, the
+// first level holding <= arity^llv nodes, copied to d_out and zero-filled to arity^llv nodes
+// (4 words each) — the level that openings of that depth are checked against.
+extern "C" uint64_t b200_tree_last_level_words(uint64_t arity, uint64_t last_level_verification)
+{
+    uint64_t n = 1;
+    for (uint64_t i = 0; i < last_level_verification; i++) n *= arity;
+    return 4 * n;
+}
+
+extern "C" int b200_tree_last_level_device(uint64_t *d_out, const uint64_t *d_tree, uint64_t NExt, uint64_t arity,
+                                           uint64_t last_level_verification, void *stream)
+{
+    if (arity < 2 || arity > 4 || last_level_verification == 0 || last_level_verification > 32)
+        return set_err(B200_EINVAL, "arity 2..4 and last_level_verification >= 1 required");
+    if (!d_out || !d_tree) return set_err(B200_EINVAL, "null buffer");
+    const uint64_t stop = b200_tree_last_level_words(arity, last_level_verification) / 4;
+    uint64_t n = NExt, offset = 0;
+    while (n > stop) {
+        n = (n + arity - 1) / arity;
+        offset += n * arity * 4;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaMemcpyAsync(d_out, d_tree + offset, n * 4 * 8, cudaMemcpyDeviceToDevice, s), "level copy");
+    if (stop > n) CK(cudaMemsetAsync(d_out + n * 4, 0, (stop - n) * 4 * 8, s), "level zero fill");
+    return B200_OK;
+}
+
+// merkletreeReduce (poseidon2_goldilocks.hpp merkletreeReduce; W = 4 * arity): the tree levels
+// above n given digests (d_digests, 4 words each), in d_tree (b200_tree_num_elements(n, arity)
+// words, level 0 = a copy of the digests), with the native hash family; the root to root_host.
+extern "C" int b200_merkletree_reduce_device(uint64_t *root_host, const uint64_t *d_digests, uint64_t n,
+                                             uint64_t arity, uint64_t *d_tree, void *stream)
+{
+    if (arity < 2 || arity > 4) return set_err(B200_EINVAL, "arity must be 2, 3 or 4");
+    if (n == 0 || !d_digests || !d_tree) return set_err(B200_EINVAL, "empty digest list or null buffer");
+    int rc = ensure_init_current();
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaMemcpyAsync(d_tree, d_digests, n * 4 * 8, cudaMemcpyDeviceToDevice, s), "digests copy");
+    const int fam = g_native_family.load();
+    cudaError_t e;
+    switch (arity) {
+    case 2: e = fam == 1 ? merkle::build_levels<8, 1>(d_tree, n, s) : merkle::build_levels<8, 2>(d_tree, n, s); break;
+    case 3: e = fam == 1 ? merkle::build_levels<12, 1>(d_tree, n, s) : merkle::build_levels<12, 2>(d_tree, n, s); break;
+    default: e = fam == 1 ? merkle::build_levels<16, 1>(d_tree, n, s) : merkle::build_levels<16, 2>(d_tree, n, s); break;
+    }
+    CK(e, "tree levels");
+    if (root_host) {
+        const uint64_t total = merkle::tree_num_elements(n, arity);
+        CK(cudaMemcpyAsync(root_host, d_tree + total - 4, 32, cudaMemcpyDeviceToHost, s), "root D2H");
+        CK(cudaStreamSynchronize(s), "sync");
+    }
+    return B200_OK;
+}

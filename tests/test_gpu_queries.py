@@ -78,3 +78,71 @@ def test_openings_zero_queries_and_bad_arity(dev, torch_cuda):
     with pytest.raises(dev.B200Error):
         dev.query_openings_device(d_out, d_lde, 128, 4, d_tree, 5, d_rows, 1)
     assert dev.query_proof_words(128, 4, 4, 0) == 4 + 4 * 3 * 4  # 128 -> 32 -> 8 -> 2 -> 1: 4 levels
+
+
+def _verify_to_level(orc, opening, ncols, nrows, arity, row, level, llv):
+    """verifyGroupProof with last_level_verification (merkleTreeGL.cpp:177-216): the row's linear
+    hash combined with the siblings up to the kept level, compared with that level's node."""
+    w = 4 * arity
+    h = orc.linear_hash(w, opening[:ncols])
+    sib = opening[ncols:]
+    idx, n, stop = row, nrows, arity ** llv
+    while n > stop:
+        cur = idx % arity
+        st = np.zeros(w, dtype=np.uint64)
+        p = 0
+        for i in range(arity):
+            if i == cur:
+                st[4 * i:4 * i + 4] = h
+            else:
+                st[4 * i:4 * i + 4] = sib[4 * p:4 * p + 4]
+                p += 1
+        sib = sib[4 * (arity - 1):]
+        h = orc.permute(st)[:4]
+        idx //= arity
+        n = (n + arity - 1) // arity
+    return (h == level[4 * idx:4 * idx + 4]).all()
+
+
+@pytest.mark.parametrize("nbits,nbe,ncols,arity", [(8, 9, 7, 4), (9, 10, 3, 2), (8, 10, 12, 3)])
+def test_last_level_and_openings_verify(dev, torch_cuda, orc, nbits, nbe, ncols, arity):
+    torch = torch_cuda
+    trace, d_lde, d_tree, root = _commit(dev, torch, nbits, nbe, ncols, arity, 70 + nbits)
+    next_ = 1 << nbe
+    lde = from_dev(d_lde)[: next_ * ncols].reshape(ncols, next_).T.copy()
+    tree = from_dev(d_tree)
+    for llv in (1, 2, 3):
+        words = dev.load().b200_tree_last_level_words(arity, llv)
+        d_level = torch.full((words,), -1, dtype=torch.int64, device="cuda")
+        dev.tree_last_level_device(d_level, d_tree, next_, arity, llv)
+        torch.cuda.synchronize()
+        level = from_dev(d_level)
+        # restatement of getLevel over the host copy of the tree
+        n, off = next_, 0
+        while n > arity ** llv:
+            n = (n + arity - 1) // arity
+            off += n * arity * 4
+        exp = np.zeros(words, dtype=np.uint64)
+        exp[:4 * n] = tree[off:off + 4 * n]
+        assert (level == exp).all(), llv
+        for row in (0, 3, next_ - 1):
+            opening = orc.group_proof(lde, tree, arity, row, llv)
+            assert _verify_to_level(orc, opening, ncols, next_, arity, row, level, llv), (llv, row)
+
+
+@pytest.mark.parametrize("n,arity", [(1, 4), (5, 2), (12, 3), (100, 4), (4097, 2)])
+def test_merkletree_reduce_device(dev, torch_cuda, orc, refcpu, n, arity):
+    torch = torch_cuda
+    digests = oracle.random_field((4 * n,), n + arity)
+    d_tree = torch.zeros(dev.tree_num_elements(n, arity), dtype=torch.int64, device="cuda")
+    root = dev.merkletree_reduce_device(to_dev(torch, digests), n, arity, d_tree)
+    assert (root == orc.merkletree_reduce(4 * arity, digests, arity)).all()
+    assert (root == refcpu.merkletree_reduce(4 * arity, digests, arity)).all()
+
+
+def test_merkletree_reduce_golden(dev, torch_cuda, kats):
+    torch = torch_cuda
+    digests = np.arange(1, 13, dtype=np.uint64)
+    d_tree = torch.zeros(dev.tree_num_elements(3, 3), dtype=torch.int64, device="cuda")
+    root = dev.merkletree_reduce_device(to_dev(torch, digests), 3, 3, d_tree)
+    assert [int(v) for v in root] == kats["poseidon2"]["MERKLETREE_REDUCE_W12_AR3_GOLDEN"]
