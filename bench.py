@@ -578,13 +578,142 @@ def run_serving(args):
     return 0
 
 
+def run_extras(args):
+    """Throughput of the commit's consumers and variants at realistic sizes (one JSON line):
+    Q-stage commit (computeQ + tree), FRI query openings from a resident commit, bit-packed,
+    indexed and streaming commits.  Inputs resident on the device except the streaming commit,
+    whose packed rows are read from pinned host memory as the reference's slot commit does."""
+    import torch
+
+    pkg = load_package()
+    pkg.init(0)
+    dev = torch.device("cuda", 0)
+    s = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ev0.record(s)
+        for _ in range(reps):
+            fn()
+        ev1.record(s)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / reps
+
+    def breakdown(fn):
+        """per-category device ms of one untimed call (the unpack kernels count as transpose)"""
+        torch.cuda.synchronize()
+        pkg.timing_reset()
+        pkg.timing_enable(True)
+        try:
+            fn()
+            torch.cuda.synchronize()
+            return {k: round(v[0], 3) for k, v in pkg.timing().items() if v[1]}
+        finally:
+            pkg.timing_enable(False)
+
+    out = {}
+    # Q stage: N = 2^22, NExt = 2^23, qDeg 2, qDim 3 (cubic extension limbs)
+    nb, nbe, qdeg, qdim = 22, 23, 2, 3
+    q = torch.empty((1 << nbe) * qdim, dtype=torch.int64, device=dev)
+    pkg.fill_random_device(q, q.numel(), 11, s)
+    cmq = torch.empty((1 << nbe) * qdeg * qdim, dtype=torch.int64, device=dev)
+    qtree = torch.empty(pkg.tree_num_elements(1 << nbe, 4), dtype=torch.int64, device=dev)
+    qscr = torch.empty(pkg.q_scratch_words(nbe, qdim), dtype=torch.int64, device=dev)
+    ms = timed(lambda: pkg.commit_q_device(cmq, qtree, q, nb, nbe, qdeg, qdim, 4, qscr, stream=s), args.steps)
+    out["q_stage"] = {"shape": "N 2^22 -> NExt 2^23, qDeg 2 x qDim 3, arity 4", "ms": round(ms, 3),
+                      "gelem_s": round((1 << nbe) * qdeg * qdim / ms / 1e6, 3),
+                      "kernel_ms": breakdown(lambda: pkg.commit_q_device(cmq, qtree, q, nb, nbe, qdeg, qdim, 4, qscr,
+                                                                         stream=s))}
+    del q, cmq, qtree, qscr
+    # query openings: 2^19 x 256 commit, 2^20-row tree, 1024 queries
+    nb, nbe, nc = 19, 20, 256
+    tr = torch.empty((1 << nb) * nc, dtype=torch.int64, device=dev)
+    pkg.fill_random_device(tr, tr.numel(), 12, s)
+    lde = torch.empty((1 << nbe) * nc, dtype=torch.int64, device=dev)
+    tree = torch.empty(pkg.tree_num_elements(1 << nbe, 4), dtype=torch.int64, device=dev)
+    scr = torch.empty((1 << nb) * nc, dtype=torch.int64, device=dev)
+    pkg.commit_device(lde, tree, tr, nb, nbe, nc, 4, scr, stream=s)
+    nq = 1024
+    rows = torch.from_numpy((np.random.default_rng(5).integers(0, 1 << nbe, nq)).astype(np.int64)).to(dev)
+    words = pkg.query_proof_words(1 << nbe, nc, 4)
+    opn = torch.empty(nq * words, dtype=torch.int64, device=dev)
+    ms = timed(lambda: pkg.query_openings_device(opn, lde, 1 << nbe, nc, tree, 4, rows, nq, stream=s), 20)
+    out["query_openings"] = {"shape": "1024 openings of 2^20-row x 256-column commit (%d words each)" % words,
+                             "ms": round(ms, 4), "openings_per_s": round(nq / ms * 1e3, 1)}
+    del tr, lde, tree, scr, opn
+    # packed commit: 2^22 x 64 columns of 32 bits (half the plain trace's bytes)
+    nb, nbe, nc, wbits = 22, 23, 64, 32
+    bits = [wbits] * nc
+    wpr = pkg.packed_words_per_row(bits)
+    packed = torch.empty((1 << nb) * wpr, dtype=torch.int64, device=dev)
+    pkg.fill_random_device(packed, packed.numel(), 13, s)
+    lde = torch.empty((1 << nbe) * nc, dtype=torch.int64, device=dev)
+    tree = torch.empty(pkg.tree_num_elements(1 << nbe, 4), dtype=torch.int64, device=dev)
+    scr = torch.empty((1 << nb) * nc, dtype=torch.int64, device=dev)
+    ms = timed(lambda: pkg.commit_packed_device(lde, tree, packed, wpr, bits, nb, nbe, 4, scr, stream=s), args.steps)
+    out["packed_commit"] = {"shape": "2^22 x 64 columns x 32 bits, blowup 2", "ms": round(ms, 3),
+                            "gelem_s": round((1 << nbe) * nc / ms / 1e6, 3),
+                            "kernel_ms": breakdown(lambda: pkg.commit_packed_device(lde, tree, packed, wpr, bits, nb,
+                                                                                    nbe, 4, scr, stream=s))}
+    tr = torch.empty((1 << nb) * nc, dtype=torch.int64, device=dev)
+    pkg.fill_random_device(tr, tr.numel(), 17, s)
+    ms = timed(lambda: pkg.commit_device(lde, tree, tr, nb, nbe, nc, 4, scr, stream=s), args.steps)
+    out["plain_commit_same_shape"] = {"shape": "2^22 x 64 columns, row-major u64 trace, blowup 2", "ms": round(ms, 3),
+                                      "gelem_s": round((1 << nbe) * nc / ms / 1e6, 3),
+                                      "kernel_ms": breakdown(lambda: pkg.commit_device(lde, tree, tr, nb, nbe, nc, 4,
+                                                                                       scr, stream=s))}
+    del tr
+    # indexed commit: same shape, half the columns from a 256-entry instruction table
+    src = [c % 2 for c in range(nc)]
+    ib, ent = 8, 256
+    rt_bits = sum(b for b, x in zip(bits, src) if not x) + ib
+    wpr_i = (rt_bits + 63) // 64
+    wpe = (sum(b for b, x in zip(bits, src) if x) + 63) // 64
+    rows_i = torch.empty((1 << nb) * wpr_i, dtype=torch.int64, device=dev)
+    pkg.fill_random_device(rows_i, rows_i.numel(), 14, s)
+    table = torch.empty(ent * wpe, dtype=torch.int64, device=dev)
+    pkg.fill_random_device(table, table.numel(), 15, s)
+    ms = timed(lambda: pkg.commit_indexed_device(lde, tree, rows_i, wpr_i, table, ent, wpe, ib, bits, src, nb, nbe,
+                                                 4, scr, stream=s), args.steps)
+    out["indexed_commit"] = {"shape": "2^22 x 64 columns x 32 bits (32 from a 256-entry table), blowup 2",
+                             "ms": round(ms, 3), "gelem_s": round((1 << nbe) * nc / ms / 1e6, 3),
+                             "kernel_ms": breakdown(lambda: pkg.commit_indexed_device(
+                                 lde, tree, rows_i, wpr_i, table, ent, wpe, ib, bits, src, nb, nbe, 4, scr,
+                                 stream=s))}
+    del packed, lde, tree, scr, rows_i, table
+    torch.cuda.empty_cache()
+    # streaming slot commit (Poseidon1, as the reference's slot commit): 2^20 x 64 x 32 bits from host
+    nb, nbe = 20, 21
+    host_rows = torch.empty((1 << nb) * wpr, dtype=torch.int64, pin_memory=True)
+    pkg.load().b200_fill_random_host(host_rows.data_ptr(), host_rows.numel(), 16)
+    hp = host_rows.numpy().view(np.uint64).reshape(1 << nb, wpr)
+    nbytes = pkg.stream_commit_slot_bytes(nb, nbe, nc, wpr)
+    slot = torch.empty(nbytes // 8, dtype=torch.int64, device=dev)
+    pkg.set_native_hash_family(1)
+    try:
+        ms = timed(lambda: pkg.stream_commit_packed(slot, nbytes // 8, hp, bits, nb, nbe, stream=s), args.steps)
+    finally:
+        pkg.set_native_hash_family(2)
+    out["stream_commit"] = {"shape": "2^20 x 64 columns x 32 bits from pinned host rows, blowup 2, Poseidon1 W16, "
+                                     "slot %.2f GB" % (nbytes / 1e9), "ms": round(ms, 3),
+                            "gelem_s": round((1 << nbe) * nc / ms / 1e6, 3)}
+    line = {"metric": "commit consumers and variants (Q stage, query openings, packed / indexed / streaming "
+                      "commits)", "workload": "extras", "unit": "mixed", "results": out, "n_gpus": 1,
+            "dtype": "u64", "data": "synthetic (seeded uniform words)"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c3", "c3small", "c5"], default="c2")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["c3", "c3small", "c5", "extras"], default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--budget-gb", type=float, default=120.0, help="device memory per wave (c3, c3small)")
@@ -604,6 +733,8 @@ def main():
         return run_batched(args)
     if args.workload == "c5":
         return run_serving(args)
+    if args.workload == "extras":
+        return run_extras(args)
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         return run_reference(args, wl)
