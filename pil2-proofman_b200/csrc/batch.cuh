@@ -12,6 +12,7 @@
 // and the whole sequence is captured once in a CUDA graph and replayed (BatchPlan).
 // Every kernel body is the plain path's body, so results are bit-identical to it.
 #pragma once
+#include <array>
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -83,8 +84,9 @@ __global__ void __launch_bounds__(512, 2) pass_grouped(const PassEntry *e, int n
     ntt::pass16_body(p, local % tiles, local / tiles);
 }
 
-// Grouped fixed-shape window: every entry of the launch has window shape (K, LGL).
-template <int K, int LGL>
+// Grouped fixed-shape window: every entry of the launch has window shape (K, LGL) and
+// direction DIF.
+template <int K, int LGL, bool DIF>
 __global__ void __launch_bounds__(ntt::Shape<K, LGL>::NT, 1024 / ntt::Shape<K, LGL>::NT)
     pass_fixed_grouped(const PassEntry *e, int n)
 {
@@ -92,35 +94,36 @@ __global__ void __launch_bounds__(ntt::Shape<K, LGL>::NT, 1024 / ntt::Shape<K, L
     const uint64_t local = blockIdx.x - e[i].begin;
     const uint64_t tiles = e[i].tiles;
     const ntt::Pass p = e[i].p;
-    ntt::pass_fixed_body<K, LGL>(p, (uint32_t)(local % tiles), local / tiles);
+    ntt::pass_fixed_body<K, LGL, DIF>(p, (uint32_t)(local % tiles), local / tiles);
 }
 
 typedef void (*GroupedKernel)(const PassEntry *, int);
 
 template <int K>
-inline GroupedKernel grouped_fixed_k(uint32_t lgL)
+inline GroupedKernel grouped_fixed_k(uint32_t lgL, uint32_t dif)
 {
-    if (lgL == 13 - K) return pass_fixed_grouped<K, 13 - K>;
-    if (lgL == 0) return pass_fixed_grouped<K, 0>;
+    if (lgL == 13 - K) return dif ? pass_fixed_grouped<K, 13 - K, true> : pass_fixed_grouped<K, 13 - K, false>;
+    if (lgL == 0) return dif ? pass_fixed_grouped<K, 0, true> : pass_fixed_grouped<K, 0, false>;
     return nullptr;
 }
 
-// the grouped fixed-shape kernel of a window shape, or null (the generic grouped kernel serves it)
-inline GroupedKernel grouped_fixed(uint32_t k, uint32_t lgL)
+// the grouped fixed-shape kernel of a window shape and direction, or null (the generic grouped
+// kernel serves it)
+inline GroupedKernel grouped_fixed(uint32_t k, uint32_t lgL, uint32_t dif)
 {
     switch (k) {
-    case 1: return grouped_fixed_k<1>(lgL);
-    case 2: return grouped_fixed_k<2>(lgL);
-    case 3: return grouped_fixed_k<3>(lgL);
-    case 4: return grouped_fixed_k<4>(lgL);
-    case 5: return grouped_fixed_k<5>(lgL);
-    case 6: return grouped_fixed_k<6>(lgL);
-    case 7: return grouped_fixed_k<7>(lgL);
-    case 8: return grouped_fixed_k<8>(lgL);
-    case 9: return grouped_fixed_k<9>(lgL);
-    case 10: return grouped_fixed_k<10>(lgL);
-    case 11: return grouped_fixed_k<11>(lgL);
-    case 12: return grouped_fixed_k<12>(lgL);
+    case 1: return grouped_fixed_k<1>(lgL, dif);
+    case 2: return grouped_fixed_k<2>(lgL, dif);
+    case 3: return grouped_fixed_k<3>(lgL, dif);
+    case 4: return grouped_fixed_k<4>(lgL, dif);
+    case 5: return grouped_fixed_k<5>(lgL, dif);
+    case 6: return grouped_fixed_k<6>(lgL, dif);
+    case 7: return grouped_fixed_k<7>(lgL, dif);
+    case 8: return grouped_fixed_k<8>(lgL, dif);
+    case 9: return grouped_fixed_k<9>(lgL, dif);
+    case 10: return grouped_fixed_k<10>(lgL, dif);
+    case 11: return grouped_fixed_k<11>(lgL, dif);
+    case 12: return grouped_fixed_k<12>(lgL, dif);
     default: return nullptr;
     }
 }
@@ -129,13 +132,15 @@ inline cudaError_t set_grouped_fixed_attrs()
 {
     for (uint32_t k = 1; k <= NTT_KMAX; k++) {
         const uint32_t shapes[2] = {13 - k, 0};
-        for (uint32_t lgL : shapes) {
-            GroupedKernel g = grouped_fixed(k, lgL);
-            if (!g) continue;
-            const uint32_t T = 1u << (k + lgL);
-            cudaError_t e = cudaFuncSetAttribute(g, cudaFuncAttributeMaxDynamicSharedMemorySize, (T + T / 16) * 8);
-            if (e != cudaSuccess) return e;
-        }
+        for (uint32_t lgL : shapes)
+            for (uint32_t dif = 0; dif < 2; dif++) {
+                GroupedKernel g = grouped_fixed(k, lgL, dif);
+                if (!g) continue;
+                const uint32_t T = 1u << (k + lgL);
+                cudaError_t e =
+                    cudaFuncSetAttribute(g, cudaFuncAttributeMaxDynamicSharedMemorySize, (T + T / 16) * 8);
+                if (e != cudaSuccess) return e;
+            }
     }
     return cudaSuccess;
 }
@@ -179,13 +184,14 @@ __global__ void gather_roots(const uint64_t *const *tree_ends, int n, uint64_t *
 // ------------------------------------------------------------------ host plan ----
 
 struct Launch {
-    int kind;  // 0 transpose, 1 pass (generic), 2 leaf, 3 node, 5 pass (fixed shape width, lgl)
+    int kind;  // 0 transpose, 1 pass (generic), 2 leaf, 3 node, 5 pass (fixed shape width, lgl, dif)
     int width;
     size_t off;  // byte offset of the entry array in the device table buffer
     int n;
     uint64_t blocks;
     size_t smem;
     int lgl = 0;
+    int dif = 0;
 };
 
 class Plan {
@@ -213,35 +219,36 @@ class Plan {
         h_roots = nullptr;
     }
 
-    // one window index's entries as launches: one per fixed window shape, the rest generic
+    // one window index's entries as launches: one per fixed window shape and direction, the
+    // rest generic
     void push_passes(const std::vector<PassEntry> &pe)
     {
-        std::vector<std::pair<uint32_t, uint32_t>> shapes;
+        std::vector<std::array<uint32_t, 3>> shapes;
         for (const PassEntry &e : pe) {
-            const std::pair<uint32_t, uint32_t> sh{e.p.k, e.p.lgL};
-            if (grouped_fixed(sh.first, sh.second) &&
-                std::find(shapes.begin(), shapes.end(), sh) == shapes.end())
+            const std::array<uint32_t, 3> sh{e.p.k, e.p.lgL, e.p.dif ? 1u : 0u};
+            if (grouped_fixed(sh[0], sh[1], sh[2]) && std::find(shapes.begin(), shapes.end(), sh) == shapes.end())
                 shapes.push_back(sh);
         }
         for (const auto &sh : shapes) {
             std::vector<PassEntry> g;
             uint64_t b = 0;
             for (PassEntry e : pe)
-                if (e.p.k == sh.first && e.p.lgL == sh.second) {
+                if (e.p.k == sh[0] && e.p.lgL == sh[1] && (e.p.dif ? 1u : 0u) == sh[2]) {
                     e.begin = b;
                     b += e.tiles * e.ncols;
                     g.push_back(e);
                 }
-            const size_t T = 1ull << (sh.first + sh.second);
-            Launch L{5, (int)sh.first, push(g), (int)g.size(), b, (T + T / 16) * 8};
-            L.lgl = (int)sh.second;
+            const size_t T = 1ull << (sh[0] + sh[1]);
+            Launch L{5, (int)sh[0], push(g), (int)g.size(), b, (T + T / 16) * 8};
+            L.lgl = (int)sh[1];
+            L.dif = (int)sh[2];
             launches.push_back(L);
         }
         std::vector<PassEntry> rest;
         uint64_t b = 0;
         size_t smem = 0;
         for (PassEntry e : pe)
-            if (!grouped_fixed(e.p.k, e.p.lgL)) {
+            if (!grouped_fixed(e.p.k, e.p.lgL, e.p.dif)) {
                 e.begin = b;
                 b += e.tiles * e.ncols;
                 const size_t T = 1ull << (e.p.k + e.p.lgL);
@@ -442,7 +449,7 @@ class Plan {
             case 5: {
                 const uint32_t T = 1u << (L.width + L.lgl);
                 const uint32_t nt = T / 16 < 32 ? 32 : T / 16 > 512 ? 512 : T / 16;
-                grouped_fixed((uint32_t)L.width, (uint32_t)L.lgl)<<<(unsigned)L.blocks, nt, L.smem, s>>>(
+                grouped_fixed((uint32_t)L.width, (uint32_t)L.lgl, (uint32_t)L.dif)<<<(unsigned)L.blocks, nt, L.smem, s>>>(
                     (const PassEntry *)ent, L.n);
                 break;
             }

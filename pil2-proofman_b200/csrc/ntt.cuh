@@ -372,8 +372,10 @@ __device__ __forceinline__ void phases_fixed(uint64_t *sm)
     }
 }
 
-// One CTA of Shape<K,LGL>::NT threads: tile `tile` of column `col` of the window `a`.
-template <int K, int LGL>
+// One CTA of Shape<K,LGL>::NT threads: tile `tile` of column `col` of the window `a`, whose
+// direction (a.dif) is DIF.  The direction is a template parameter so that each instantiation
+// holds only its own load path and twiddle placement.
+template <int K, int LGL, bool DIF>
 __device__ __forceinline__ void pass_fixed_body(const Pass &a, uint32_t tile, uint64_t col)
 {
     extern __shared__ uint64_t sm[];
@@ -386,7 +388,7 @@ __device__ __forceinline__ void pass_fixed_body(const Pass &a, uint32_t tile, ui
     const uint32_t base = (hi << (s0 + K)) | (lob << LGL);
     const uint64_t *S = a.src + col * a.src_cs;
     uint64_t *D = a.dst + col * a.dst_cs;
-    const bool inv = a.dif != 0;
+    constexpr bool inv = DIF;
     const uint32_t tw_shift = NTT_TWLG - s0 - K;
     const uint32_t rep = a.rep, gshift = a.gshift, goff = (uint32_t)a.goff;
 
@@ -422,7 +424,7 @@ __device__ __forceinline__ void pass_fixed_body(const Pass &a, uint32_t tile, ui
         }
     }
     __syncthreads();
-    if (inv)
+    if constexpr (inv)
         phases_fixed<true, K, LGL, K / NTT_PHASE_BITS>(sm);
     else
         phases_fixed<false, K, LGL, 0>(sm);
@@ -448,39 +450,40 @@ __device__ __forceinline__ void pass_fixed_body(const Pass &a, uint32_t tile, ui
     }
 }
 
-template <int K, int LGL>
+template <int K, int LGL, bool DIF>
 __global__ void __launch_bounds__(Shape<K, LGL>::NT, 1024 / Shape<K, LGL>::NT) pass_fixed_kernel(Pass a)
 {
-    pass_fixed_body<K, LGL>(a, blockIdx.x, blockIdx.y);
+    pass_fixed_body<K, LGL, DIF>(a, blockIdx.x, blockIdx.y);
 }
 
 typedef void (*PassKernel)(Pass);
 
-// Instantiated shapes: full 8192-element tiles (K + LGL = 13: every window of a large
-// transform but the inverse's first) and single-lane windows (LGL = 0: the inverse's first).
+// Instantiated shapes, each in both directions: full 8192-element tiles (K + LGL = 13: every
+// window of a large transform but the inverse's first) and single-lane windows (LGL = 0: the
+// inverse's first).
 template <int K>
-inline PassKernel fixed_kernel_k(uint32_t lgL)
+inline PassKernel fixed_kernel_k(uint32_t lgL, uint32_t dif)
 {
-    if (lgL == 13 - K) return pass_fixed_kernel<K, 13 - K>;
-    if (lgL == 0) return pass_fixed_kernel<K, 0>;
+    if (lgL == 13 - K) return dif ? pass_fixed_kernel<K, 13 - K, true> : pass_fixed_kernel<K, 13 - K, false>;
+    if (lgL == 0) return dif ? pass_fixed_kernel<K, 0, true> : pass_fixed_kernel<K, 0, false>;
     return nullptr;
 }
 
-inline PassKernel fixed_kernel(uint32_t k, uint32_t lgL)
+inline PassKernel fixed_kernel(uint32_t k, uint32_t lgL, uint32_t dif)
 {
     switch (k) {
-    case 1: return fixed_kernel_k<1>(lgL);
-    case 2: return fixed_kernel_k<2>(lgL);
-    case 3: return fixed_kernel_k<3>(lgL);
-    case 4: return fixed_kernel_k<4>(lgL);
-    case 5: return fixed_kernel_k<5>(lgL);
-    case 6: return fixed_kernel_k<6>(lgL);
-    case 7: return fixed_kernel_k<7>(lgL);
-    case 8: return fixed_kernel_k<8>(lgL);
-    case 9: return fixed_kernel_k<9>(lgL);
-    case 10: return fixed_kernel_k<10>(lgL);
-    case 11: return fixed_kernel_k<11>(lgL);
-    case 12: return fixed_kernel_k<12>(lgL);
+    case 1: return fixed_kernel_k<1>(lgL, dif);
+    case 2: return fixed_kernel_k<2>(lgL, dif);
+    case 3: return fixed_kernel_k<3>(lgL, dif);
+    case 4: return fixed_kernel_k<4>(lgL, dif);
+    case 5: return fixed_kernel_k<5>(lgL, dif);
+    case 6: return fixed_kernel_k<6>(lgL, dif);
+    case 7: return fixed_kernel_k<7>(lgL, dif);
+    case 8: return fixed_kernel_k<8>(lgL, dif);
+    case 9: return fixed_kernel_k<9>(lgL, dif);
+    case 10: return fixed_kernel_k<10>(lgL, dif);
+    case 11: return fixed_kernel_k<11>(lgL, dif);
+    case 12: return fixed_kernel_k<12>(lgL, dif);
     default: return nullptr;
     }
 }
@@ -490,13 +493,15 @@ inline cudaError_t set_fixed_attrs()
 {
     for (uint32_t k = 1; k <= NTT_KMAX; k++) {
         const uint32_t shapes[2] = {13 - k, 0};
-        for (uint32_t lgL : shapes) {
-            PassKernel kf = fixed_kernel(k, lgL);
-            if (!kf) continue;
-            const uint32_t T = 1u << (k + lgL);
-            cudaError_t e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (T + T / 16) * 8);
-            if (e != cudaSuccess) return e;
-        }
+        for (uint32_t lgL : shapes)
+            for (uint32_t dif = 0; dif < 2; dif++) {
+                PassKernel kf = fixed_kernel(k, lgL, dif);
+                if (!kf) continue;
+                const uint32_t T = 1u << (k + lgL);
+                cudaError_t e =
+                    cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (T + T / 16) * 8);
+                if (e != cudaSuccess) return e;
+            }
     }
     return cudaSuccess;
 }
@@ -612,7 +617,7 @@ inline cudaError_t launch_pass(const Pass &p, uint64_t ncols, cudaStream_t strea
     if (threads > 512) threads = 512;
     dim3 grid((unsigned)tiles, (unsigned)ncols);
     const size_t smem = (size_t)(T + T / 16) * 8;
-    if (PassKernel kf = fixed_kernel(p.k, p.lgL)) {
+    if (PassKernel kf = fixed_kernel(p.k, p.lgL, p.dif)) {
         kf<<<grid, threads, smem, stream>>>(p);
     } else {
         pass16_kernel<<<grid, threads, smem, stream>>>(p);
