@@ -6,8 +6,13 @@
 // four words followed by adding the four column sums (poseidon2_goldilocks.hpp:201-240).
 //
 // The linear layers run on 96-bit accumulators (all coefficients are small and
-// positive, so a row of M_E is below 80 * 2^64) and are reduced once per output word;
-// the partial-round update x_i*D_i + sum is one 128-bit multiply-add and one reduction.
+// positive) and are reduced once per output word: by linearity M_E x = M4(block) + M4(S)
+// with S the column sums of the blocks, so each output is M4(block) + M4(S) (+ the next
+// full round's constants, folded in before the reduction) < 33 * 2^64.  The partial-round
+// update x_i*D_i + sum is one 128-bit multiply-add and one reduction, and the next round's sum
+// of x_1.. is accumulated while they are updated.  Against the form that reduced M4(block)
+// first, added the reduced column sums and reduced again, and re-read x_1.. for every partial
+// round's sum, this is 6 % more W16 permutations per second (B200).
 // All state words are loose (< 2^64, congruent mod p); the round constants are canonical.
 #pragma once
 #include "gl64.cuh"
@@ -65,34 +70,46 @@ __device__ __forceinline__ void m4(uint64_t a, uint64_t b, uint64_t c, uint64_t 
 // warps together with a barrier per round was measured too and gave nothing.)
 // ---------------------------------------------------------------------------------
 
+// M_E x = M4(block) + M4(sum of the blocks) (linearity), plus the next round's constants cn
+// (canonical; null: none) before the single reduction of each output.
 template <int W, int TPB>
-__device__ __forceinline__ void external_layer_smem(uint64_t *st)
+__device__ __forceinline__ void external_layer_smem(uint64_t *st, const uint64_t *cn)
 {
-    gl::Acc s0 = {0, 0, 0}, s1 = {0, 0, 0}, s2 = {0, 0, 0}, s3 = {0, 0, 0};
+    gl::Acc S0 = gl::acc_add6464(st[0 * TPB], st[4 * TPB]), S1 = gl::acc_add6464(st[1 * TPB], st[5 * TPB]),
+            S2 = gl::acc_add6464(st[2 * TPB], st[6 * TPB]), S3 = gl::acc_add6464(st[3 * TPB], st[7 * TPB]);
+#pragma unroll
+    for (int q = 8; q < W; q += 4) {
+        S0 = gl::acc_add64(S0, st[(q + 0) * TPB]);
+        S1 = gl::acc_add64(S1, st[(q + 1) * TPB]);
+        S2 = gl::acc_add64(S2, st[(q + 2) * TPB]);
+        S3 = gl::acc_add64(S3, st[(q + 3) * TPB]);
+    }
+    gl::Acc t0, t1, t2, t3;
+    m4(gl::acc_reduce(S0), gl::acc_reduce(S1), gl::acc_reduce(S2), gl::acc_reduce(S3), t0, t1, t2, t3);
 #pragma unroll 1
     for (int q = 0; q < W; q += 4) {
         gl::Acc y0, y1, y2, y3;
         m4(st[(q + 0) * TPB], st[(q + 1) * TPB], st[(q + 2) * TPB], st[(q + 3) * TPB], y0, y1, y2, y3);
-        s0 = gl::acc_add(s0, y0);
-        s1 = gl::acc_add(s1, y1);
-        s2 = gl::acc_add(s2, y2);
-        s3 = gl::acc_add(s3, y3);
+        y0 = gl::acc_add(y0, t0);
+        y1 = gl::acc_add(y1, t1);
+        y2 = gl::acc_add(y2, t2);
+        y3 = gl::acc_add(y3, t3);
+        if (cn) {
+            y0 = gl::acc_add64(y0, cn[q + 0]);
+            y1 = gl::acc_add64(y1, cn[q + 1]);
+            y2 = gl::acc_add64(y2, cn[q + 2]);
+            y3 = gl::acc_add64(y3, cn[q + 3]);
+        }
         st[(q + 0) * TPB] = gl::acc_reduce(y0);
         st[(q + 1) * TPB] = gl::acc_reduce(y1);
         st[(q + 2) * TPB] = gl::acc_reduce(y2);
         st[(q + 3) * TPB] = gl::acc_reduce(y3);
     }
-    const uint64_t t0 = gl::acc_reduce(s0), t1 = gl::acc_reduce(s1), t2 = gl::acc_reduce(s2),
-                   t3 = gl::acc_reduce(s3);
-#pragma unroll 1
-    for (int q = 0; q < W; q += 4) {
-        st[(q + 0) * TPB] = gl::acc_reduce(gl::acc_add6464(st[(q + 0) * TPB], t0));
-        st[(q + 1) * TPB] = gl::acc_reduce(gl::acc_add6464(st[(q + 1) * TPB], t1));
-        st[(q + 2) * TPB] = gl::acc_reduce(gl::acc_add6464(st[(q + 2) * TPB], t2));
-        st[(q + 3) * TPB] = gl::acc_reduce(gl::acc_add6464(st[(q + 3) * TPB], t3));
-    }
 }
 
+// Rounds: r = 0 the initial M_E; r = 1..8 the full rounds (x^7 on every word, M_E), the 22
+// partial rounds after r = 4.  Each full round's constants are added by the linear layer before
+// it, except round 5's, which follows the partial rounds.
 template <int W, int TPB>
 __device__ __forceinline__ void permute_smem(uint64_t *st)
 {
@@ -101,41 +118,44 @@ __device__ __forceinline__ void permute_smem(uint64_t *st)
 #pragma unroll 1
     for (int r = 0; r <= 8; r++) {
         if (r > 0) {
-            const uint64_t *Cr = C + (r <= 4 ? (r - 1) * W : 4 * W + NPARTIAL + (r - 5) * W);
+            const uint64_t *Cr = r == 5 ? C + 4 * W + NPARTIAL : nullptr;
 #pragma unroll 1
             for (int q = 0; q < W; q += 4) {
                 uint64_t a = st[(q + 0) * TPB], b = st[(q + 1) * TPB], c = st[(q + 2) * TPB], d = st[(q + 3) * TPB];
-                a = gl::pow7(gl::add_c(a, Cr[q + 0]));
-                b = gl::pow7(gl::add_c(b, Cr[q + 1]));
-                c = gl::pow7(gl::add_c(c, Cr[q + 2]));
-                d = gl::pow7(gl::add_c(d, Cr[q + 3]));
-                st[(q + 0) * TPB] = a;
-                st[(q + 1) * TPB] = b;
-                st[(q + 2) * TPB] = c;
-                st[(q + 3) * TPB] = d;
+                if (Cr) {
+                    a = gl::add_c(a, Cr[q + 0]);
+                    b = gl::add_c(b, Cr[q + 1]);
+                    c = gl::add_c(c, Cr[q + 2]);
+                    d = gl::add_c(d, Cr[q + 3]);
+                }
+                st[(q + 0) * TPB] = gl::pow7(a);
+                st[(q + 1) * TPB] = gl::pow7(b);
+                st[(q + 2) * TPB] = gl::pow7(c);
+                st[(q + 3) * TPB] = gl::pow7(d);
             }
         }
-        external_layer_smem<W, TPB>(st);
+        // constants of round r + 1 (rounds 1..4: C + r * W; rounds 6..8: C + 4W + 22 + (r - 4) * W)
+        const uint64_t *cn = r < 4 ? C + r * W : (r >= 5 && r < 8 ? C + 4 * W + NPARTIAL + (r - 4) * W : nullptr);
+        external_layer_smem<W, TPB>(st, cn);
         if (r == 4) {
-            // partial rounds: x0 stays in a register; the other words stream through smem
+            // partial rounds: x0 in a register; the sum of x_1.. for the next round is
+            // accumulated while they are updated
             uint64_t x0 = st[0];
+            gl::Acc rest = gl::acc_add6464(st[1 * TPB], st[2 * TPB]);
+#pragma unroll
+            for (int i = 3; i < W; i++) rest = gl::acc_add64(rest, st[i * TPB]);
 #pragma unroll 1
             for (int pr = 0; pr < NPARTIAL; pr++) {
                 x0 = gl::pow7(gl::add_c(x0, C[4 * W + pr]));
-                gl::Acc s = gl::acc(x0);
-#pragma unroll 1
-                for (int q = 4; q < W + 4; q += 4) {
-                    const int i = q - 4;
-                    if (i) s = gl::acc_add64(s, st[(i + 0) * TPB]);
-                    s = gl::acc_add64(s, st[(i + 1) * TPB]);
-                    s = gl::acc_add64(s, st[(i + 2) * TPB]);
-                    s = gl::acc_add64(s, st[(i + 3) * TPB]);
-                }
-                const uint64_t sum = gl::acc_reduce(s);
+                const uint64_t sum = gl::acc_reduce(gl::acc_add64(rest, x0));
                 x0 = gl::mul_add(x0, D[0], sum);
-                st[1 * TPB] = gl::mul_add(st[1 * TPB], D[1], sum);
-                st[2 * TPB] = gl::mul_add(st[2 * TPB], D[2], sum);
-                st[3 * TPB] = gl::mul_add(st[3 * TPB], D[3], sum);
+                const uint64_t u1 = gl::mul_add(st[1 * TPB], D[1], sum);
+                const uint64_t u2 = gl::mul_add(st[2 * TPB], D[2], sum);
+                const uint64_t u3 = gl::mul_add(st[3 * TPB], D[3], sum);
+                st[1 * TPB] = u1;
+                st[2 * TPB] = u2;
+                st[3 * TPB] = u3;
+                rest = gl::acc_add64(gl::acc_add6464(u1, u2), u3);
 #pragma unroll 1
                 for (int q = 4; q < W; q += 4) {
                     const uint64_t a = gl::mul_add(st[(q + 0) * TPB], D[q + 0], sum);
@@ -146,6 +166,7 @@ __device__ __forceinline__ void permute_smem(uint64_t *st)
                     st[(q + 1) * TPB] = b;
                     st[(q + 2) * TPB] = c;
                     st[(q + 3) * TPB] = d;
+                    rest = gl::acc_add64(gl::acc_add64(gl::acc_add64(gl::acc_add64(rest, a), b), c), d);
                 }
             }
             st[0] = x0;
