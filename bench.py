@@ -601,16 +601,23 @@ def run_extras(args):
     s = torch.cuda.current_stream()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    def timed(fn, reps):
+    spread = {}
+
+    def timed(fn, reps, name=None):
+        """mean ms per call over reps calls (CUDA events on s); per-call min/max kept in spread"""
         for _ in range(args.warmup):
             fn()
         torch.cuda.synchronize()
-        ev0.record(s)
-        for _ in range(reps):
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(reps + 1)]
+        evs[0].record(s)
+        for i in range(reps):
             fn()
-        ev1.record(s)
+            evs[i + 1].record(s)
         torch.cuda.synchronize()
-        return ev0.elapsed_time(ev1) / reps
+        per = [evs[i].elapsed_time(evs[i + 1]) for i in range(reps)]
+        if name:
+            spread[name] = [round(min(per), 3), round(max(per), 3)]
+        return evs[0].elapsed_time(evs[reps]) / reps
 
     def breakdown(fn):
         """per-category device ms of one untimed call (the unpack kernels count as transpose)"""
@@ -663,14 +670,16 @@ def run_extras(args):
     lde = torch.empty((1 << nbe) * nc, dtype=torch.int64, device=dev)
     tree = torch.empty(pkg.tree_num_elements(1 << nbe, 4), dtype=torch.int64, device=dev)
     scr = torch.empty((1 << nb) * nc, dtype=torch.int64, device=dev)
-    ms = timed(lambda: pkg.commit_packed_device(lde, tree, packed, wpr, bits, nb, nbe, 4, scr, stream=s), args.steps)
+    ms = timed(lambda: pkg.commit_packed_device(lde, tree, packed, wpr, bits, nb, nbe, 4, scr, stream=s), args.steps,
+               "packed_commit")
     out["packed_commit"] = {"shape": "2^22 x 64 columns x 32 bits, blowup 2", "ms": round(ms, 3),
                             "gelem_s": round((1 << nbe) * nc / ms / 1e6, 3),
                             "kernel_ms": breakdown(lambda: pkg.commit_packed_device(lde, tree, packed, wpr, bits, nb,
                                                                                     nbe, 4, scr, stream=s))}
     tr = torch.empty((1 << nb) * nc, dtype=torch.int64, device=dev)
     pkg.fill_random_device(tr, tr.numel(), 17, s)
-    ms = timed(lambda: pkg.commit_device(lde, tree, tr, nb, nbe, nc, 4, scr, stream=s), args.steps)
+    ms = timed(lambda: pkg.commit_device(lde, tree, tr, nb, nbe, nc, 4, scr, stream=s), args.steps,
+               "plain_commit_same_shape")
     out["plain_commit_same_shape"] = {"shape": "2^22 x 64 columns, row-major u64 trace, blowup 2", "ms": round(ms, 3),
                                       "gelem_s": round((1 << nbe) * nc / ms / 1e6, 3),
                                       "kernel_ms": breakdown(lambda: pkg.commit_device(lde, tree, tr, nb, nbe, nc, 4,
@@ -687,7 +696,7 @@ def run_extras(args):
     table = torch.empty(ent * wpe, dtype=torch.int64, device=dev)
     pkg.fill_random_device(table, table.numel(), 15, s)
     ms = timed(lambda: pkg.commit_indexed_device(lde, tree, rows_i, wpr_i, table, ent, wpe, ib, bits, src, nb, nbe,
-                                                 4, scr, stream=s), args.steps)
+                                                 4, scr, stream=s), args.steps, "indexed_commit")
     out["indexed_commit"] = {"shape": "2^22 x 64 columns x 32 bits (32 from a 256-entry table), blowup 2",
                              "ms": round(ms, 3), "gelem_s": round((1 << nbe) * nc / ms / 1e6, 3),
                              "kernel_ms": breakdown(lambda: pkg.commit_indexed_device(
@@ -712,7 +721,7 @@ def run_extras(args):
                             "gelem_s": round((1 << nbe) * nc / ms / 1e6, 3)}
     line = {"metric": "commit consumers and variants (Q stage, query openings, packed / indexed / streaming "
                       "commits)", "workload": "extras", "unit": "mixed", "results": out, "n_gpus": 1,
-            "dtype": "u64", "data": "synthetic (seeded uniform words)"}
+            "dtype": "u64", "data": "synthetic (seeded uniform words)", "per_call_min_max_ms": spread}
     print(json.dumps(line), flush=True)
     return 0
 

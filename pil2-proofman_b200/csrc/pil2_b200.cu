@@ -279,6 +279,7 @@ extern "C" const char *b200_kernel_names(void)
     return "pass16_kernel\ntranspose_kernel\nleaf_hash_kernel\nnode_kernel\npermute_kernel\nlde_rows_kernel\n"
            "fill_kernel\nimad_probe_kernel\ntranspose_grouped\npass_grouped\nleaf_persistent\n"
            "node_grouped\ngather_roots\npass_fixed_kernel\nopenings_kernel\nunpack_kernel\nunpack_indexed_kernel\n"
+           "unpack_indexed_param_kernel\n"
            "unpack_range_kernel\nabsorb_kernel\npass_fixed_grouped\n";
 }
 
@@ -1035,7 +1036,7 @@ extern "C" int b200_commit_packed_device(uint64_t *root_host, uint64_t *d_lde, u
     if (nCols && !col_bits) return set_err(B200_EINVAL, "null column widths");
     for (uint64_t c = 0; c < nCols; c++)
         if (col_bits[c] < 1 || col_bits[c] > 64) return set_err(B200_EINVAL, "column width outside 1..64");
-    if (nCols > 12288) return set_err(B200_EINVAL, "packed commit supports at most 12288 columns");
+    if (nCols > unpack::COLS_MAX) return set_err(B200_EINVAL, "packed commit supports at most 12288 columns");
     if (nCols && words_per_row * 64 < unpack::packed_bits(col_bits, nCols))
         return set_err(B200_EINVAL, "words_per_row too small for the column widths");
     if ((rc = ensure_init_current())) return rc;
@@ -1043,18 +1044,15 @@ extern "C" int b200_commit_packed_device(uint64_t *root_host, uint64_t *d_lde, u
     const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
     if (!d_tree || (nCols && (!d_lde || !d_packed || !d_scratch))) return set_err(B200_EINVAL, "null buffer");
     if (nCols) {
-        uint32_t *d_bits = nullptr;
-        CK(cudaMallocAsync((void **)&d_bits, nCols * 4, s), "column widths buffer");
-        CK(cudaMemcpyAsync(d_bits, col_bits, nCols * 4, cudaMemcpyHostToDevice, s), "column widths H2D");
+        unpack::ColBytes cols;  // widths in the kernel parameters
+        for (uint64_t c = 0; c < nCols; c++) cols.v[c] = (uint8_t)col_bits[c];
         {
             prof::Scope ps(prof::TRANSPOSE, s);
-            unpack::unpack_kernel<<<(unsigned)((N + 255) / 256), 256, nCols * 4, s>>>(d_scratch, d_packed, N, nCols,
-                                                                                     words_per_row, d_bits);
+            unpack::unpack_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(d_scratch, d_packed, N, nCols,
+                                                                             words_per_row, cols);
             prof::count();
         }
-        const cudaError_t e = cudaGetLastError();
-        cudaFreeAsync(d_bits, s);
-        CK(e, "unpack");
+        CK(cudaGetLastError(), "unpack");
         // the trace now sits column-major in the scratch; the LDE transforms it in place
         CK(ntt::lde(d_lde, d_scratch, false, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, d_scratch, s), "lde");
     }
@@ -1332,6 +1330,7 @@ extern "C" int b200_commit_indexed_device(uint64_t *root_host, uint64_t *d_lde, 
     int rc = check_shape(nBits, nBitsExt, nCols, arity);
     if (rc) return rc;
     if (nCols && (!col_bits || !col_source)) return set_err(B200_EINVAL, "null column description");
+    if (nCols > unpack::COLS_MAX) return set_err(B200_EINVAL, "indexed commit supports at most 12288 columns");
     std::vector<uint64_t> info(nCols);
     const IndexedDesc ix{col_source, index_bits, d_table, num_entries, words_per_entry};
     if (nCols && (rc = indexed_info(info.data(), col_bits, nCols, words_per_row, ix))) return rc;
@@ -1340,19 +1339,16 @@ extern "C" int b200_commit_indexed_device(uint64_t *root_host, uint64_t *d_lde, 
     const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
     if (!d_tree || (nCols && (!d_lde || !d_rows || !d_scratch))) return set_err(B200_EINVAL, "null buffer");
     if (nCols) {
-        uint64_t *d_info = nullptr;
-        CK(cudaMallocAsync((void **)&d_info, nCols * 8, s), "column info buffer");
-        CK(cudaMemcpyAsync(d_info, info.data(), nCols * 8, cudaMemcpyHostToDevice, s), "column info H2D");
+        unpack::ColBytes cols;  // width | table source << 7 per column, in the kernel parameters
+        for (uint64_t c = 0; c < nCols; c++) cols.v[c] = (uint8_t)((info[c] & 127) | ((info[c] >> 32) << 7));
         {
             prof::Scope ps(prof::TRANSPOSE, s);
-            unpack::unpack_indexed_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(
-                d_scratch, d_rows, d_table, N, words_per_row, words_per_entry, num_entries, index_bits, d_info, 0,
+            unpack::unpack_indexed_param_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(
+                d_scratch, d_rows, d_table, N, words_per_row, words_per_entry, num_entries, index_bits, cols, 0,
                 (uint32_t)nCols);
             prof::count();
         }
-        const cudaError_t e = cudaGetLastError();
-        cudaFreeAsync(d_info, s);
-        CK(e, "indexed unpack");
+        CK(cudaGetLastError(), "indexed unpack");
         CK(ntt::lde(d_lde, d_scratch, false, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, d_scratch, s), "lde");
     }
     CK(merkle::build_tree_arity(arity, d_tree, d_lde, 1, NExt, nCols, NExt, s, g_native_family.load()), "merkletree");

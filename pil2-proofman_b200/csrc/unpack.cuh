@@ -12,19 +12,24 @@
 
 namespace unpack {
 
+// Column descriptions passed by value in the kernel parameters (no device allocation or copy
+// per call): one byte per column, width 1..64 in bits 0-6, table source (indexed witness) in
+// bit 7.  12 KB, inside the 32 KB kernel-parameter limit.
+constexpr uint32_t COLS_MAX = 12288;
+struct ColBytes {
+    uint8_t v[COLS_MAX];
+};
+
 __global__ void __launch_bounds__(256) unpack_kernel(uint64_t *__restrict__ dst, const uint64_t *__restrict__ src,
                                                      uint64_t nrows, uint64_t ncols, uint64_t words_per_row,
-                                                     const uint32_t *__restrict__ col_bits)
+                                                     const __grid_constant__ ColBytes cols)
 {
-    extern __shared__ uint32_t bits_sm[];
-    for (uint64_t c = threadIdx.x; c < ncols; c += blockDim.x) bits_sm[c] = col_bits[c];
-    __syncthreads();
     const uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (row >= nrows) return;
     const uint64_t *w = src + row * words_per_row;
     uint64_t word = words_per_row ? __ldg(w) : 0, idx = 0, off = 0;
     for (uint64_t c = 0; c < ncols; c++) {
-        const uint32_t nb = bits_sm[c];
+        const uint32_t nb = cols.v[c] & 127u;
         uint64_t val;
         const uint64_t left = 64 - off;
         if (nb <= left) {
@@ -81,19 +86,30 @@ struct Cursor {
     }
 };
 
+// Column info of the indexed kernels: width | source << 32, from device memory (the streaming
+// slot's table) or from the kernel parameters.
+struct InfoDev {
+    const uint64_t *p;
+};
+__device__ __forceinline__ uint64_t col_info(const InfoDev &t, uint32_t c) { return __ldg(t.p + c); }
+__device__ __forceinline__ uint64_t col_info(const ColBytes &t, uint32_t c)
+{
+    const uint32_t b = t.v[c];
+    return (uint64_t)(b & 127u) | ((uint64_t)(b >> 7) << 32);
+}
+
 // Indexed witness (the reference's unpack_indexed, starks_gpu.cu:125-185): a row is a leading
-// instruction index (index_bits wide) followed by the runtime columns; the columns flagged in
-// col_info (bit 32) are read instead from entry `index` of a shared instruction table
+// instruction index (index_bits wide) followed by the runtime columns; the columns flagged as
+// table columns are read instead from entry `index` of a shared instruction table
 // (words_per_entry words per entry, its own bit cursor).  An index past the table selects entry
-// 0, as the reference does.  col_info[c] = width | source << 32.  Columns [c0, c0 + cc) are
-// written (column-major, stride nrows); earlier columns only advance the cursors.
-__global__ void __launch_bounds__(256) unpack_indexed_kernel(uint64_t *__restrict__ dst,
-                                                             const uint64_t *__restrict__ rows,
-                                                             const uint64_t *__restrict__ table, uint64_t nrows,
-                                                             uint64_t words_per_row, uint64_t words_per_entry,
-                                                             uint64_t num_entries, uint64_t index_bits,
-                                                             const uint64_t *__restrict__ col_info, uint32_t c0,
-                                                             uint32_t cc)
+// 0, as the reference does.  Columns [c0, c0 + cc) are written (column-major, stride nrows);
+// earlier columns only advance the cursors.
+template <class Info>
+__device__ __forceinline__ void unpack_indexed_body(uint64_t *__restrict__ dst, const uint64_t *__restrict__ rows,
+                                                    const uint64_t *__restrict__ table, uint64_t nrows,
+                                                    uint64_t words_per_row, uint64_t words_per_entry,
+                                                    uint64_t num_entries, uint64_t index_bits, const Info &info,
+                                                    uint32_t c0, uint32_t cc)
 {
     const uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (row >= nrows) return;
@@ -103,14 +119,45 @@ __global__ void __launch_bounds__(256) unpack_indexed_kernel(uint64_t *__restric
     if (index >= num_entries) index = 0;
     t.start(table + index * words_per_entry, words_per_entry);
     for (uint32_t c = 0; c < c0 + cc; c++) {
-        const uint64_t info = __ldg(col_info + c), nb = info & 0xffffffffull;
-        Cursor &k = (info >> 32) ? t : r;
-        if (c < c0) {
-            k.take<false>(nb);
+        const uint64_t ci = col_info(info, c), nb = ci & 0xffffffffull;
+        if (ci >> 32) {
+            if (c < c0)
+                t.take<false>(nb);
+            else
+                dst[(uint64_t)(c - c0) * nrows + row] = t.take<true>(nb);
         } else {
-            dst[(uint64_t)(c - c0) * nrows + row] = k.take<true>(nb);
+            if (c < c0)
+                r.take<false>(nb);
+            else
+                dst[(uint64_t)(c - c0) * nrows + row] = r.take<true>(nb);
         }
     }
+}
+
+// col_info in device memory (width | source << 32 per column)
+__global__ void __launch_bounds__(256) unpack_indexed_kernel(uint64_t *__restrict__ dst,
+                                                             const uint64_t *__restrict__ rows,
+                                                             const uint64_t *__restrict__ table, uint64_t nrows,
+                                                             uint64_t words_per_row, uint64_t words_per_entry,
+                                                             uint64_t num_entries, uint64_t index_bits,
+                                                             const uint64_t *__restrict__ col_info, uint32_t c0,
+                                                             uint32_t cc)
+{
+    unpack_indexed_body(dst, rows, table, nrows, words_per_row, words_per_entry, num_entries, index_bits,
+                        InfoDev{col_info}, c0, cc);
+}
+
+// column bytes in the kernel parameters
+__global__ void __launch_bounds__(256) unpack_indexed_param_kernel(uint64_t *__restrict__ dst,
+                                                                   const uint64_t *__restrict__ rows,
+                                                                   const uint64_t *__restrict__ table, uint64_t nrows,
+                                                                   uint64_t words_per_row, uint64_t words_per_entry,
+                                                                   uint64_t num_entries, uint64_t index_bits,
+                                                                   const __grid_constant__ ColBytes cols, uint32_t c0,
+                                                                   uint32_t cc)
+{
+    unpack_indexed_body(dst, rows, table, nrows, words_per_row, words_per_entry, num_entries, index_bits, cols, c0,
+                        cc);
 }
 
 // bits of a packed row (host check of words_per_row)
