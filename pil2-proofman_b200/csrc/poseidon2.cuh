@@ -7,8 +7,9 @@
 //
 // The linear layers run on 96-bit accumulators (all coefficients are small and
 // positive) and are reduced once per output word: by linearity M_E x = M4(block) + M4(S)
-// with S the column sums of the blocks, so each output is M4(block) + M4(S) (+ the next
-// full round's constants, folded in before the reduction) < 33 * 2^64.  The partial-round
+// with S the column sums of the blocks (M4(S) taken on the unreduced 96-bit sums), so each
+// output is M4(block) + M4(S) (+ the next full round's constants, folded in before the
+// reduction) < 81 * 2^64.  The partial-round
 // update x_i*D_i + sum is one 128-bit multiply-add and one reduction, and the next round's sum
 // of x_1.. is accumulated while they are updated.  Against the form that reduced M4(block)
 // first, added the reduced column sums and reduced again, and re-read x_1.. for every partial
@@ -61,6 +62,24 @@ __device__ __forceinline__ void m4(uint64_t a, uint64_t b, uint64_t c, uint64_t 
     y3 = r3;
 }
 
+// M4 on 96-bit inputs (each below 2^92): 96-bit outputs (coefficient sums <= 16)
+__device__ __forceinline__ void m4_acc(gl::Acc a, gl::Acc b, gl::Acc c, gl::Acc d, gl::Acc &y0, gl::Acc &y1,
+                                       gl::Acc &y2, gl::Acc &y3)
+{
+    gl::Acc ab = gl::acc_add(a, b);
+    gl::Acc cd = gl::acc_add(c, d);
+    gl::Acc bbcd = gl::acc_add(gl::acc_add(b, b), cd);
+    gl::Acc ddab = gl::acc_add(gl::acc_add(d, d), ab);
+    gl::Acc cd2 = gl::acc_add(cd, cd);
+    gl::Acc ab2 = gl::acc_add(ab, ab);
+    gl::Acc r3 = gl::acc_add(gl::acc_add(cd2, cd2), ddab);
+    gl::Acc r1 = gl::acc_add(gl::acc_add(ab2, ab2), bbcd);
+    y0 = gl::acc_add(ddab, r1);
+    y1 = r1;
+    y2 = gl::acc_add(bbcd, r3);
+    y3 = r3;
+}
+
 // ---------------------------------------------------------------------------------
 // The permutation keeps each thread's W state words in shared memory at st[i*TPB] (TPB
 // threads interleaved: a warp touches 32 consecutive words, no bank conflicts) and runs
@@ -85,7 +104,7 @@ __device__ __forceinline__ void external_layer_smem(uint64_t *st, const uint64_t
         S3 = gl::acc_add64(S3, st[(q + 3) * TPB]);
     }
     gl::Acc t0, t1, t2, t3;
-    m4(gl::acc_reduce(S0), gl::acc_reduce(S1), gl::acc_reduce(S2), gl::acc_reduce(S3), t0, t1, t2, t3);
+    m4_acc(S0, S1, S2, S3, t0, t1, t2, t3);
 #pragma unroll 1
     for (int q = 0; q < W; q += 4) {
         gl::Acc y0, y1, y2, y3;
