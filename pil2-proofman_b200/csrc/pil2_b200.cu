@@ -280,7 +280,8 @@ extern "C" const char *b200_kernel_names(void)
            "fill_kernel\nimad_probe_kernel\ntranspose_grouped\npass_grouped\nleaf_persistent\n"
            "node_grouped\ngather_roots\npass_fixed_kernel\nopenings_kernel\nunpack_kernel\nunpack_indexed_kernel\n"
            "unpack_indexed_param_kernel\n"
-           "unpack_range_kernel\nabsorb_kernel\npass_fixed_grouped\n";
+           "unpack_range_kernel\nabsorb_kernel\npass_fixed_grouped\nnode_coop_kernel\ntree_tail_kernel\n"
+           "leaf_coop_kernel\n";
 }
 
 // ------------------------------------------------------------ host-buffer API ----
