@@ -77,11 +77,17 @@ __global__ void __launch_bounds__(256) transpose_grouped(const TransposeEntry *e
 
 __global__ void __launch_bounds__(512, 2) pass_grouped(const PassEntry *e, int n)
 {
-    const int i = find_entry(e, n, blockIdx.x);
-    const uint64_t local = blockIdx.x - e[i].begin;
-    const uint64_t tiles = e[i].tiles;
-    const ntt::Pass p = e[i].p;
-    ntt::pass16_body(p, local % tiles, local / tiles);
+    __shared__ ntt::Pass p;  // staged like pass_fixed_grouped's
+    __shared__ uint32_t tile, col;
+    if (threadIdx.x == 0) {
+        const int i = find_entry(e, n, blockIdx.x);
+        p = e[i].p;
+        const uint32_t local = (uint32_t)(blockIdx.x - e[i].begin), tiles = (uint32_t)e[i].tiles;
+        tile = local % tiles;
+        col = local / tiles;
+    }
+    __syncthreads();
+    ntt::pass16_body(p, tile, col);
 }
 
 // Grouped fixed-shape window: every entry of the launch has window shape (K, LGL) and
@@ -90,11 +96,20 @@ template <int K, int LGL, bool DIF>
 __global__ void __launch_bounds__(ntt::Shape<K, LGL>::NT, 1024 / ntt::Shape<K, LGL>::NT)
     pass_fixed_grouped(const PassEntry *e, int n)
 {
-    const int i = find_entry(e, n, blockIdx.x);
-    const uint64_t local = blockIdx.x - e[i].begin;
-    const uint64_t tiles = e[i].tiles;
-    const ntt::Pass p = e[i].p;
-    ntt::pass_fixed_body<K, LGL, DIF>(p, (uint32_t)(local % tiles), local / tiles);
+    // the entry's window description staged in shared memory (read there as needed, not held in
+    // registers: a register copy of the struct pushed the window bodies into spills)
+    __shared__ ntt::Pass p;
+    __shared__ uint32_t tile, col;
+    if (threadIdx.x == 0) {
+        const int i = find_entry(e, n, blockIdx.x);
+        p = e[i].p;
+        // block and tile counts of a launch are below 2^31
+        const uint32_t local = (uint32_t)(blockIdx.x - e[i].begin), tiles = (uint32_t)e[i].tiles;
+        tile = local % tiles;
+        col = local / tiles;
+    }
+    __syncthreads();
+    ntt::pass_fixed_body<K, LGL, DIF>(p, tile, col);
 }
 
 typedef void (*GroupedKernel)(const PassEntry *, int);
@@ -152,16 +167,18 @@ __global__ void __launch_bounds__(merkle::TPB, merkle::Family<FAM>::MIN_CTAS)
 {
     __shared__ uint64_t sm[merkle::Family<FAM>::SMEM_AREAS * W * merkle::TPB];
     __shared__ uint64_t claim;
+    __shared__ LeafEntry L;  // the claimed block's instance, staged for the CTA
     for (;;) {
-        if (threadIdx.x == 0) claim = atomicAdd(counter, 1ull);
+        if (threadIdx.x == 0) {
+            claim = atomicAdd(counter, 1ull);
+            if (claim < total) L = e[find_entry(e, n, claim)];
+        }
         __syncthreads();
         const uint64_t b = claim;
-        __syncthreads();
         if (b >= total) return;
-        const int i = find_entry(e, n, b);
-        const LeafEntry L = e[i];
         const uint64_t row = (b - L.begin) * merkle::TPB + threadIdx.x;
         if (row < L.nrows) merkle::leaf_row<W, FAM>(sm + threadIdx.x, L.digests, L.src, 1, L.nrows, L.ncols, row);
+        __syncthreads();
     }
 }
 
