@@ -57,13 +57,13 @@ __device__ __forceinline__ uint64_t shfl_u64(uint64_t x, int src)
     return gl::mk64(lo, hi);
 }
 
+// the three low 32-bit words of an accumulator (values < 2^96)
 __device__ __forceinline__ gl::Acc shfl_xor_acc(gl::Acc a, int m)
 {
-    gl::Acc r;
-    r.w0 = __shfl_xor_sync(0xffffffffu, a.w0, m);
-    r.w1 = __shfl_xor_sync(0xffffffffu, a.w1, m);
-    r.w2 = __shfl_xor_sync(0xffffffffu, a.w2, m);
-    return r;
+    const uint32_t w0 = __shfl_xor_sync(0xffffffffu, (uint32_t)a.v, m);
+    const uint32_t w1 = __shfl_xor_sync(0xffffffffu, (uint32_t)(a.v >> 32), m);
+    const uint32_t w2 = __shfl_xor_sync(0xffffffffu, (uint32_t)(a.v >> 64), m);
+    return gl::Acc{((unsigned __int128)w2 << 64) | ((unsigned __int128)w1 << 32) | w0};
 }
 
 // sum of a over the lanes that differ from this one only in lane bits [LO_BIT, HI_BIT) (xor
@@ -101,16 +101,7 @@ __device__ __forceinline__ gl::Acc dot4(const Row &m, uint64_t a0, uint64_t a1, 
     asm("mad.wide.u32 %0, %1, %2, %0;" : "+l"(H) : "r"(gl::hi32(a1)), "r"(m.m1));
     asm("mad.wide.u32 %0, %1, %2, %0;" : "+l"(H) : "r"(gl::hi32(a2)), "r"(m.m2));
     asm("mad.wide.u32 %0, %1, %2, %0;" : "+l"(H) : "r"(gl::hi32(a3)), "r"(m.m3));
-    // L + H * 2^32 (L, H < 2^37)
-    gl::Acc r;
-    uint32_t c;
-    r.w0 = gl::lo32(L);
-    asm("add.cc.u32 %0, %2, %3;\n\t"
-        "addc.u32   %1, 0, 0;\n\t"
-        : "=r"(r.w1), "=r"(c)
-        : "r"(gl::hi32(L)), "r"(gl::lo32(H)));
-    r.w2 = gl::hi32(H) + c;
-    return r;
+    return gl::acc_lohi(L, H);  // L, H < 2^37
 }
 
 // M_E on the group's state: lane k (block k/4, row k%4) gets M4(block)_k%4 + sum over the blocks
@@ -122,7 +113,7 @@ __device__ __forceinline__ uint64_t external_layer(uint64_t x, int gbase, int k,
     const int b0 = gbase + (k & ~3);
     const uint64_t a0 = shfl_u64(x, b0), a1 = shfl_u64(x, b0 + 1), a2 = shfl_u64(x, b0 + 2), a3 = shfl_u64(x, b0 + 3);
     gl::Acc y = dot4(row, a0, a1, a2, a3);
-    if (!live) y = gl::Acc{0, 0, 0};
+    if (!live) y = gl::Acc{0};
     const gl::Acc t = xor_sum<2, (G == 16 ? 4 : 3)>(y);
     return gl::acc_reduce(gl::acc_add(y, t));
 }

@@ -231,55 +231,36 @@ __device__ __forceinline__ uint64_t pow7(uint64_t x)
     return mul(x3, x4);
 }
 
-// ---- 96-bit accumulators for linear layers with small positive coefficients ----
+// ---- accumulators for linear layers with small positive coefficients ----
+// Sums of a few dozen loose words times small coefficients stay below 2^96.  They are kept as
+// 128-bit integers: the compiler's carry chains for these adds measured 1.8 % faster over a
+// Poseidon2 permutation than hand-written three-word add.cc chains.
 struct Acc {
-    uint32_t w0, w1, w2;
+    unsigned __int128 v;
 };
 
-__device__ __forceinline__ Acc acc(uint64_t a) { return Acc{lo32(a), hi32(a), 0u}; }
-
-__device__ __forceinline__ Acc acc_add(Acc a, Acc b)
+__device__ __forceinline__ Acc acc(uint64_t a) { return Acc{(unsigned __int128)a}; }
+__device__ __forceinline__ Acc acc_add(Acc a, Acc b) { return Acc{a.v + b.v}; }
+__device__ __forceinline__ Acc acc_add64(Acc a, uint64_t b) { return Acc{a.v + b}; }
+__device__ __forceinline__ Acc acc_add6464(uint64_t a, uint64_t b) { return Acc{(unsigned __int128)a + b}; }
+// lo + hi * 2^32 for lo, hi < 2^64 - 2^32 (two 64-bit sums of 32x32 products over the low and
+// high halves of the inputs)
+__device__ __forceinline__ Acc acc_lohi(uint64_t lo, uint64_t hi)
 {
-    Acc r;
-    asm("add.cc.u32  %0, %3, %6;\n\t"
-        "addc.cc.u32 %1, %4, %7;\n\t"
-        "addc.u32    %2, %5, %8;\n\t"
-        : "=r"(r.w0), "=r"(r.w1), "=r"(r.w2)
-        : "r"(a.w0), "r"(a.w1), "r"(a.w2), "r"(b.w0), "r"(b.w1), "r"(b.w2));
-    return r;
+    return Acc{(unsigned __int128)lo + ((unsigned __int128)hi << 32)};
 }
 
-__device__ __forceinline__ Acc acc_add64(Acc a, uint64_t b)
-{
-    Acc r;
-    asm("add.cc.u32  %0, %3, %5;\n\t"
-        "addc.cc.u32 %1, %4, %6;\n\t"
-        "addc.u32    %2, %7, 0;\n\t"
-        : "=r"(r.w0), "=r"(r.w1), "=r"(r.w2)
-        : "r"(a.w0), "r"(a.w1), "r"(lo32(b)), "r"(hi32(b)), "r"(a.w2));
-    return r;
-}
-
-__device__ __forceinline__ Acc acc_add6464(uint64_t a, uint64_t b)
-{
-    Acc r;
-    asm("add.cc.u32  %0, %3, %5;\n\t"
-        "addc.cc.u32 %1, %4, %6;\n\t"
-        "addc.u32    %2, 0, 0;\n\t"
-        : "=r"(r.w0), "=r"(r.w1), "=r"(r.w2)
-        : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
-    return r;
-}
-
-// fold (w2:w1:w0) = lo + w2*2^64 = lo + w2*(2^32-1): a single carry may remain, worth EPS
+// fold (w2:lo) = lo + w2*2^64 = lo + w2*(2^32-1) for w2 < 2^32: a single carry may remain, worth EPS
 __device__ __forceinline__ uint64_t acc_reduce(Acc a)
 {
+    const uint64_t lo = (uint64_t)a.v;
+    const uint32_t w2 = (uint32_t)(a.v >> 64);
     uint32_t z0, z1, c;
     asm("mad.lo.cc.u32  %0, %5, 0xffffffff, %3;\n\t"
         "madc.hi.cc.u32 %1, %5, 0xffffffff, %4;\n\t"
         "addc.u32       %2, 0, 0;\n\t"
         : "=r"(z0), "=r"(z1), "=r"(c)
-        : "r"(a.w0), "r"(a.w1), "r"(a.w2));
+        : "r"(lo32(lo)), "r"(hi32(lo)), "r"(w2));
     uint32_t m = 0u - c;
     asm("add.cc.u32  %0, %0, %2;\n\t"
         "addc.u32    %1, %1, 0;\n\t"

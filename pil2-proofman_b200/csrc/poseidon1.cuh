@@ -124,17 +124,8 @@ __device__ __forceinline__ void mvp_small(uint64_t *st, uint64_t *tmp)
         }
 #pragma unroll
         for (int u = 0; u < PASS; u++) {
-            const uint64_t l = f64_u52(L[u]), h = f64_u52(H[u]);
-            // l + h * 2^32 as three words (l, h < 2^41)
-            gl::Acc a;
-            uint32_t c;
-            a.w0 = gl::lo32(l);
-            asm("add.cc.u32 %0, %2, %3;\n\t"
-                "addc.u32   %1, 0, 0;\n\t"
-                : "=r"(a.w1), "=r"(c)
-                : "r"(gl::hi32(l)), "r"(gl::lo32(h)));
-            a.w2 = gl::hi32(h) + c;
-            tmp[(i0 + u) * TPB] = gl::acc_reduce(a);
+            // l + h * 2^32 (l, h < 2^41)
+            tmp[(i0 + u) * TPB] = gl::acc_reduce(gl::acc_lohi(f64_u52(L[u]), f64_u52(H[u])));
         }
         asm volatile("" ::: "memory");  // keep the next pass's loads after this pass's stores
     }
