@@ -15,6 +15,7 @@
 #include "../../include/pil2_b200.h"
 #include "merkle.cuh"
 #include "ntt.cuh"
+#include "stream.cuh"
 #include "synth.cuh"
 
 // ------------------------------------------------------------------ errors ----
@@ -558,6 +559,15 @@ static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_
         CK(cudaEventRecord(s.blocks[k], s.copy), "event");
     }
     CK(cudaEventRecord(s.h2d_done, s.copy), "event");
+    // With an earlier commit still running, this commit's copy hides under it and its kernels
+    // wait for it anyway.  With the device idle the copy is exposed, so an arity-4 commit hashes
+    // its rows while the later column blocks are still crossing: the row sponge in 12-column
+    // chunks (stream::absorb_kernel, the 4-word state carried in tree level 0), each chunk as
+    // soon as its columns are extended.  Same sponge, same digests.
+    const int fam = g_hash_family.load();
+    const bool idle = !b->last_end || cudaEventQuery(b->last_end) == cudaSuccess;
+    const bool chunked = idle && arity == 4 && nblk > 1;
+    uint64_t next_chunk = 0;
     if (b->last_end && b->last_end != s.end) CK(cudaStreamWaitEvent(s.stream, b->last_end, 0), "order commits");
     for (uint64_t k = 0; k < nblk; k++) {
         const uint64_t c0 = k * B, cb = (nCols - c0) < B ? (nCols - c0) : B;
@@ -578,9 +588,31 @@ static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_
                         s.d_scratch + c0 * N, s.stream),
                "lde");
         }
+        if (chunked) {
+            const uint64_t avail = k + 1 == nblk ? nCols : c0 + cb;  // columns extended so far
+            prof::Scope ps(prof::LEAF_HASH, s.stream);
+            for (; next_chunk * stream::RATE < nCols; next_chunk++) {
+                const uint64_t a0 = next_chunk * stream::RATE;
+                const uint32_t cc = (uint32_t)std::min<uint64_t>(stream::RATE, nCols - a0);
+                if (a0 + cc > avail) break;
+                const unsigned grid = (unsigned)((NExt + merkle::TPB - 1) / merkle::TPB);
+                if (fam == 1)
+                    stream::absorb_kernel<1><<<grid, merkle::TPB, 0, s.stream>>>(s.d_tree, s.d_lde + a0 * NExt, cc,
+                                                                                 next_chunk == 0, NExt);
+                else
+                    stream::absorb_kernel<2><<<grid, merkle::TPB, 0, s.stream>>>(s.d_tree, s.d_lde + a0 * NExt, cc,
+                                                                                 next_chunk == 0, NExt);
+                prof::count();
+                CK(cudaGetLastError(), "absorb");
+            }
+        }
     }
-    CK(merkle::build_tree_arity(arity, s.d_tree, s.d_lde, 1, NExt, nCols, NExt, s.stream, g_hash_family.load()),
-       "merkletree");
+    if (chunked) {
+        const cudaError_t e = fam == 1 ? merkle::build_levels<16, 1>(s.d_tree, NExt, s.stream)
+                                       : merkle::build_levels<16, 2>(s.d_tree, NExt, s.stream);
+        CK(e, "tree levels");
+    } else
+        CK(merkle::build_tree_arity(arity, s.d_tree, s.d_lde, 1, NExt, nCols, NExt, s.stream, fam), "merkletree");
     CK(cudaMemcpyAsync(s.h_root, s.d_tree + tsz - 4, 32, cudaMemcpyDeviceToHost, s.stream), "root D2H");
     CK(cudaEventRecord(s.end, s.stream), "event");
     b->last_end = s.end;
@@ -1067,7 +1099,6 @@ extern "C" int b200_commit_packed_device(uint64_t *root_host, uint64_t *d_lde, u
 }
 
 // ------------------------------------------------------ streaming slot commit ----
-#include "stream.cuh"
 
 // Widths -> the slot's width and bit-offset tables (host staging of 2 x 64 words).
 static int stream_tables(uint64_t *tab, const uint64_t *colWidths, uint64_t nCols, uint64_t wordsPerRow)
