@@ -292,6 +292,15 @@ def run_ours(args, wl):
                "unit": "G butterfly-mul/s", "frac": round(ntt_gmul / peak_gmul, 4),
                "algorithmic": "nCols x (N/2 x log2 N + NExt/2 x log2 N) radix-2 butterflies, one multiplication "
                               "each; time = NTT window kernels only"}
+    # the row-major -> column-major transpose in front of the LDE is the one pure HBM pass
+    transpose_roof = None
+    if cats["transpose"][1] and cats["transpose"][0] > 0:
+        tr_ms = cats["transpose"][0] / cats["transpose"][1]
+        tr_gbs = 16 * N * ncols / (tr_ms * 1e-3) / 1e9
+        transpose_roof = {"bound": "hbm", "achieved": round(tr_gbs, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                          "frac": round(tr_gbs / peaks.get("hbm_gbs", 6650.0), 4),
+                          "algorithmic_bytes": "16 x N x nCols per commit (read the row-major trace, write it "
+                                               "column-major)"}
     roofline = {
         "kernel": "leaf_hash_kernel<%d,%d>" % (w, args.hash_family),
         "bound": "int32_imad",
@@ -307,6 +316,7 @@ def run_ours(args, wl):
                 "algorithmic_bytes": "8 x nCols x (N + NExt) per commit (read trace once, write LDE once)",
                 "traffic": ncu_traffic("ntt_lde", args.workload),
                 "int": ntt_int},
+        "transpose": transpose_roof,
     }
     kernel_ms = {k: round(v[0] / args.steps, 3) for k, v in cats.items()}
 
