@@ -89,6 +89,25 @@ def test_indexed_commit_equals_expanded(pkg, torch_cuda, orc, nbits, nbe, bits, 
     assert (root2 == exp).all()
 
 
+def test_indexed_commit_many_columns(pkg, torch_cuda, orc):
+    """290 columns (half from a 9-entry table): the column bytes travel in the kernel parameters."""
+    torch = torch_cuda
+    pkg.init(0)
+    nbits, nbe = 6, 7
+    bits = [(i * 13) % 64 + 1 for i in range(290)]
+    source = [i % 2 for i in range(290)]
+    trace, runtime, index, table_vals = make_indexed(nbits, bits, source, 4, 9, 290)
+    rows, table = pkg.pack_indexed(runtime, index, 4, table_vals, bits, source)
+    d_rows, d_table = to_dev(torch, rows), to_dev(torch, table)
+    n, ncols = 1 << nbits, len(bits)
+    d_lde = torch.zeros((1 << nbe) * ncols, dtype=torch.int64, device="cuda")
+    d_tree = torch.zeros(pkg.tree_num_elements(1 << nbe, 4), dtype=torch.int64, device="cuda")
+    d_scr = torch.zeros(n * ncols, dtype=torch.int64, device="cuda")
+    root = pkg.commit_indexed_device(d_lde, d_tree, d_rows, rows.shape[1], d_table, 9, table.shape[1], 4, bits,
+                                     source, nbits, nbe, 4, d_scr)
+    assert (root == orc.commit(trace, nbe, 4)[0]).all()
+
+
 def test_indexed_rejects(pkg, torch_cuda):
     torch = torch_cuda
     pkg.init(0)

@@ -97,7 +97,8 @@ def test_autotune_keeps_results_and_roundtrips(dev, torch_cuda, orc):
 
 @pytest.mark.parametrize("nbits,nbe,bits,arity", [
     (8, 9, [1, 7, 64, 33, 31, 2, 64, 17, 5], 4), (10, 12, [32] * 20, 3), (6, 7, [64], 2),
-    (11, 12, [3, 61, 40, 24, 63, 1, 1, 1, 60, 8, 13], 4)])
+    (11, 12, [3, 61, 40, 24, 63, 1, 1, 1, 60, 8, 13], 4),
+    (6, 7, [(i * 37) % 64 + 1 for i in range(300)], 4)])  # widths passed as kernel-parameter bytes
 def test_packed_commit_equals_plain(dev, torch_cuda, orc, nbits, nbe, bits, arity):
     torch = torch_cuda
     n, ncols = 1 << nbits, len(bits)
@@ -128,3 +129,5 @@ def test_packed_commit_rejects_bad_widths(dev, torch_cuda):
         dev.commit_packed_device(d, d, d, 2, [65], 4, 5, 4, d)
     with pytest.raises(dev.B200Error):  # words_per_row too small
         dev.commit_packed_device(d, d, d, 1, [40, 40], 4, 5, 4, d)
+    with pytest.raises(dev.B200Error):  # more columns than the kernel-parameter table holds
+        dev.commit_packed_device(d, d, d, 193, [1] * 12289, 4, 5, 4, d)
