@@ -517,11 +517,18 @@ extern "C" uint64_t gen_device_streams(void *d_buffers, uint64_t n_streams, uint
     return b->slots.size();
 }
 
-// Column blocks of the pipelined commit: 64 columns (512-byte row segments, which a 2-D copy
-// moves at full PCIe rate) when the trace is large enough for the overlap to matter.
-static uint64_t commit_block_cols(uint64_t nBits, uint64_t nCols)
+// Column blocks of the pipelined commit, as start columns (starts.back() == nCols): when the
+// trace is large enough for the overlap to matter, a 16-column first block (nothing hides its
+// copy: the kernels start once it has landed; 128-byte row segments still copy at 47 GB/s), then
+// 64-column blocks (512-byte row segments, which a 2-D copy moves at the full 55 GB/s).
+static void commit_blocks(uint64_t nBits, uint64_t nCols, std::vector<uint64_t> &starts)
 {
-    return (nBits >= 16 && nCols >= 128) ? 64 : nCols;
+    starts.assign(1, 0);
+    if (nBits >= 16 && nCols >= 128) {
+        starts.push_back(16);
+        for (uint64_t c = 64; c < nCols; c += 64) starts.push_back(c);
+    }
+    if (nCols) starts.push_back(nCols);
 }
 
 // Enqueue H2D + LDE + tree + root D2H for a row-major host trace on a slot.  The trace crosses
@@ -539,8 +546,9 @@ static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_
     if ((rc = grow(s.d_trace, s.cap_trace, N * nCols)) || (rc = grow(s.d_scratch, s.cap_scratch, N * nCols)) ||
         (rc = grow(s.d_lde, s.cap_lde, NExt * nCols)) || (rc = grow(s.d_tree, s.cap_tree, tsz)))
         return rc;
-    const uint64_t B = nCols ? commit_block_cols(nBits, nCols) : 1;
-    const uint64_t nblk = nCols ? (nCols + B - 1) / B : 0;
+    std::vector<uint64_t> starts;
+    commit_blocks(nBits, nCols, starts);
+    const uint64_t nblk = starts.size() - 1;
     while (s.blocks.size() < nblk) {
         cudaEvent_t e;
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
@@ -549,7 +557,7 @@ static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_
     // the copy may overwrite d_trace once this slot's previous commit has consumed it
     CK(cudaStreamWaitEvent(s.copy, s.end, 0), "slot reuse");
     for (uint64_t k = 0; k < nblk; k++) {
-        const uint64_t c0 = k * B, cb = (nCols - c0) < B ? (nCols - c0) : B;
+        const uint64_t c0 = starts[k], cb = starts[k + 1] - c0;
         if (cb == nCols)
             CK(cudaMemcpyAsync(s.d_trace, trace, N * nCols * 8, cudaMemcpyHostToDevice, s.copy), "trace H2D");
         else
@@ -570,7 +578,7 @@ static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_
     uint64_t next_chunk = 0;
     if (b->last_end && b->last_end != s.end) CK(cudaStreamWaitEvent(s.stream, b->last_end, 0), "order commits");
     for (uint64_t k = 0; k < nblk; k++) {
-        const uint64_t c0 = k * B, cb = (nCols - c0) < B ? (nCols - c0) : B;
+        const uint64_t c0 = starts[k], cb = starts[k + 1] - c0;
         CK(cudaStreamWaitEvent(s.stream, s.blocks[k], 0), "block landed");
         if (cb == nCols) {
             CK(ntt::lde(s.d_lde, s.d_trace, true, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, s.d_scratch, s.stream),
