@@ -1,5 +1,5 @@
-// Cooperative Poseidon2 (hash family 2) for work too small to fill the GPU with one thread
-// per state: the top levels of a tree and the leaves of tiny instances.
+// Cooperative Poseidon2 and Poseidon1 for work too small to fill the GPU with one thread per
+// state: the top levels of a tree and the leaves of tiny instances.
 //
 // One state per group of G lanes of a warp (G = 16 for W = 12 and 16, G = 8 for W = 8);
 // lane k of the group holds word k (lanes k >= W hold zero).  The S-boxes of a full round
@@ -14,6 +14,7 @@
 // identical.
 #pragma once
 #include "gl64.cuh"
+#include "poseidon1.cuh"
 #include "poseidon2_constants.h"
 
 // Round constants and diagonals in global memory: lanes read different entries, which the
@@ -24,6 +25,19 @@ __device__ uint64_t g_coop_C12[P2_NC_12] = {P2_C12_LIST};
 __device__ uint64_t g_coop_D12[12] = {P2_D12_LIST};
 __device__ uint64_t g_coop_C16[P2_NC_16] = {P2_C16_LIST};
 __device__ uint64_t g_coop_D16[16] = {P2_D16_LIST};
+// Poseidon1 (hash family 1): round constants C, small MDS M, pre-partial matrix P, sparse S
+__device__ uint64_t g_coop1_C8[P1_NC_8] = {P1_C8_LIST};
+__device__ uint64_t g_coop1_M8[64] = {P1_M8_LIST};
+__device__ uint64_t g_coop1_P8[64] = {P1_P8_LIST};
+__device__ uint64_t g_coop1_S8[P1_NS_8] = {P1_S8_LIST};
+__device__ uint64_t g_coop1_C12[P1_NC_12] = {P1_C12_LIST};
+__device__ uint64_t g_coop1_M12[144] = {P1_M12_LIST};
+__device__ uint64_t g_coop1_P12[144] = {P1_P12_LIST};
+__device__ uint64_t g_coop1_S12[P1_NS_12] = {P1_S12_LIST};
+__device__ uint64_t g_coop1_C16[P1_NC_16] = {P1_C16_LIST};
+__device__ uint64_t g_coop1_M16[256] = {P1_M16_LIST};
+__device__ uint64_t g_coop1_P16[256] = {P1_P16_LIST};
+__device__ uint64_t g_coop1_S16[P1_NS_16] = {P1_S16_LIST};
 
 namespace coop {
 
@@ -48,6 +62,30 @@ struct Tab<16> {
     static constexpr int G = 16;
     static __device__ __forceinline__ const uint64_t *C() { return g_coop_C16; }
     static __device__ __forceinline__ const uint64_t *D() { return g_coop_D16; }
+};
+
+template <int W>
+struct Tab1;
+template <>
+struct Tab1<8> {
+    static __device__ __forceinline__ const uint64_t *C() { return g_coop1_C8; }
+    static __device__ __forceinline__ const uint64_t *M() { return g_coop1_M8; }
+    static __device__ __forceinline__ const uint64_t *P() { return g_coop1_P8; }
+    static __device__ __forceinline__ const uint64_t *S() { return g_coop1_S8; }
+};
+template <>
+struct Tab1<12> {
+    static __device__ __forceinline__ const uint64_t *C() { return g_coop1_C12; }
+    static __device__ __forceinline__ const uint64_t *M() { return g_coop1_M12; }
+    static __device__ __forceinline__ const uint64_t *P() { return g_coop1_P12; }
+    static __device__ __forceinline__ const uint64_t *S() { return g_coop1_S12; }
+};
+template <>
+struct Tab1<16> {
+    static __device__ __forceinline__ const uint64_t *C() { return g_coop1_C16; }
+    static __device__ __forceinline__ const uint64_t *M() { return g_coop1_M16; }
+    static __device__ __forceinline__ const uint64_t *P() { return g_coop1_P16; }
+    static __device__ __forceinline__ const uint64_t *S() { return g_coop1_S16; }
 };
 
 __device__ __forceinline__ uint64_t shfl_u64(uint64_t x, int src)
@@ -153,6 +191,76 @@ __device__ __forceinline__ uint64_t permute(uint64_t x, int gbase, int k)
     return x;
 }
 
+// Poseidon1 matrix steps for lane k: out_k = sum_j mat[j][k] x_j over the group's words (gathered
+// by shuffles).  The small-entry M as two 64-bit sums of 32x32 products; the full-entry P in
+// 160 bits (p1::Acc160).
+template <int W>
+__device__ __forceinline__ uint64_t mvp_small1(uint64_t x, int gbase, int kk)
+{
+    const uint64_t *M = Tab1<W>::M();
+    uint64_t L = 0, H = 0;
+#pragma unroll
+    for (int j = 0; j < W; j++) {
+        const uint64_t xj = shfl_u64(x, gbase + j);
+        const uint32_t m = (uint32_t)__ldg(M + j * W + kk);
+        asm("mad.wide.u32 %0, %1, %2, %0;" : "+l"(L) : "r"(gl::lo32(xj)), "r"(m));
+        asm("mad.wide.u32 %0, %1, %2, %0;" : "+l"(H) : "r"(gl::hi32(xj)), "r"(m));
+    }
+    return gl::acc_reduce(gl::acc_lohi(L, H));
+}
+
+template <int W>
+__device__ __forceinline__ uint64_t mvp_full1(uint64_t x, int gbase, int kk)
+{
+    const uint64_t *P = Tab1<W>::P();
+    p1::Acc160 a = {{0, 0, 0, 0, 0}};
+#pragma unroll
+    for (int j = 0; j < W; j++) p1::acc160_mul_add(a, shfl_u64(x, gbase + j), __ldg(P + j * W + kk));
+    return p1::acc160_reduce(a);
+}
+
+// The Poseidon1 permutation (poseidon1.cuh's round structure: add C_0; rounds 0-3 x^7 + next
+// constants, M (P after round 3); 22 sparse partial rounds before round 4; rounds 4-7 x^7 +
+// constants (none after round 7), M) on the group's state, lane k holding word k.
+template <int W>
+__device__ __forceinline__ uint64_t permute1(uint64_t x, int gbase, int k)
+{
+    constexpr int G = Tab<W>::G;
+    const bool live = k < W;
+    const int kk = live ? k : 0;
+    const uint64_t *C = Tab1<W>::C();
+    const uint64_t *S = Tab1<W>::S();
+    x = live ? gl::add_c(x, __ldg(C + kk)) : 0ull;
+#pragma unroll 1
+    for (int r = 0; r < 8; r++) {
+        if (r == 4) {
+#pragma unroll 1
+            for (int pr = 0; pr < NPARTIAL; pr++) {
+                const uint64_t *Sr = S + (2 * W - 1) * pr;
+                const uint64_t x0 = shfl_u64(gl::add_c(gl::pow7(x), __ldg(C + 5 * W + pr)), gbase);
+                // x0' = <(x0, x_1..), Sr[0..W)>: one product per lane, summed over the group
+                const uint64_t term = live ? gl::mul(k == 0 ? x0 : x, __ldg(Sr + kk)) : 0ull;
+                const gl::Acc sum = xor_sum<0, (G == 16 ? 4 : 3)>(gl::acc(term));
+                x = k == 0 ? gl::acc_reduce(sum) : (live ? gl::mul_add(x0, __ldg(Sr + W - 1 + kk), x) : 0ull);
+            }
+        }
+        x = gl::pow7(x);
+        if (r < 7) x = gl::add_c(x, __ldg(C + (r < 4 ? (r + 1) * W : 5 * W + NPARTIAL + (r - 4) * W) + kk));
+        x = r == 3 ? mvp_full1<W>(x, gbase, kk) : mvp_small1<W>(x, gbase, kk);
+        if (!live) x = 0;
+    }
+    return x;
+}
+
+template <int W, int FAM>
+__device__ __forceinline__ uint64_t permute_fam(uint64_t x, int gbase, int k)
+{
+    if constexpr (FAM == 1)
+        return permute1<W>(x, gbase, k);
+    else
+        return permute<W>(x, gbase, k);
+}
+
 // ---------------------------------------------------------------------------------
 // Kernels.  CTAs of CTA_THREADS threads = CTA_THREADS / G states.
 // ---------------------------------------------------------------------------------
@@ -161,7 +269,7 @@ constexpr int TAIL_THREADS = 1024;
 
 // Parent i of a tree level (semantics of merkle::node_one): the W = 4 * arity child words, zero
 // past `pending`; the last parent writes the level's `pad` zero digests after its children.
-template <int W>
+template <int W, int FAM>
 __device__ __forceinline__ void node_group(uint64_t *__restrict__ level, uint64_t pending, uint64_t pad,
                                           uint64_t parents, uint64_t *__restrict__ out, uint64_t i, int gbase, int k)
 {
@@ -170,11 +278,11 @@ __device__ __forceinline__ void node_group(uint64_t *__restrict__ level, uint64_
     uint64_t x = 0;
     if (valid && k < W && i * ARITY + (uint64_t)(k >> 2) < pending) x = level[i * W + k];
     if (valid && i == parents - 1 && (uint64_t)k < pad * 4) level[pending * 4 + k] = 0;
-    x = permute<W>(x, gbase, k);
+    x = permute_fam<W, FAM>(x, gbase, k);
     if (valid && k < 4) out[i * 4 + k] = gl::canon(x);
 }
 
-template <int W>
+template <int W, int FAM = 2>
 __global__ void __launch_bounds__(CTA_THREADS) node_coop_kernel(uint64_t *__restrict__ level, uint64_t pending,
                                                                 uint64_t pad, uint64_t parents,
                                                                 uint64_t *__restrict__ out)
@@ -182,13 +290,13 @@ __global__ void __launch_bounds__(CTA_THREADS) node_coop_kernel(uint64_t *__rest
     constexpr int G = Tab<W>::G;
     const int lane = threadIdx.x & 31;
     const uint64_t i = ((uint64_t)blockIdx.x * CTA_THREADS + threadIdx.x) / G;
-    node_group<W>(level, pending, pad, parents, out, i, lane & ~(G - 1), lane & (G - 1));
+    node_group<W, FAM>(level, pending, pad, parents, out, i, lane & ~(G - 1), lane & (G - 1));
 }
 
 // Every remaining level of a tree whose current level has `pending` digests at `level`, in one
 // CTA (the level loop runs inside; a barrier separates the levels).  Used once a level has at
 // most TAIL_THREADS / G parents.
-template <int W>
+template <int W, int FAM = 2>
 __global__ void __launch_bounds__(TAIL_THREADS) tree_tail_kernel(uint64_t *level, uint64_t pending)
 {
     constexpr int G = Tab<W>::G;
@@ -199,7 +307,7 @@ __global__ void __launch_bounds__(TAIL_THREADS) tree_tail_kernel(uint64_t *level
         const uint64_t pad = (ARITY - pending % ARITY) % ARITY;
         const uint64_t parents = (pending + ARITY - 1) / ARITY;
         uint64_t *out = level + (pending + pad) * 4;
-        node_group<W>(level, pending, pad, parents, out, i, lane & ~(G - 1), lane & (G - 1));
+        node_group<W, FAM>(level, pending, pad, parents, out, i, lane & ~(G - 1), lane & (G - 1));
         __syncthreads();
         level = out;
         pending = parents;
@@ -209,7 +317,7 @@ __global__ void __launch_bounds__(TAIL_THREADS) tree_tail_kernel(uint64_t *level
 // Row sponge of row `row` (semantics of merkle::leaf_row): the capacity starts at zero; each block
 // puts the next RATE columns (zero past the last) in lanes [0, RATE) and the previous output words
 // 0..3 in the capacity lanes; the digest is words 0..3.
-template <int W>
+template <int W, int FAM = 2>
 __global__ void __launch_bounds__(CTA_THREADS) leaf_coop_kernel(uint64_t *__restrict__ digests,
                                                                 const uint64_t *__restrict__ src, uint64_t rs,
                                                                 uint64_t cs, uint64_t ncols, uint64_t nrows)
@@ -230,7 +338,7 @@ __global__ void __launch_bounds__(CTA_THREADS) leaf_coop_kernel(uint64_t *__rest
             x = done ? prev : 0ull;
         else
             x = 0;
-        x = permute<W>(x, gbase, k);
+        x = permute_fam<W, FAM>(x, gbase, k);
     }
     if (valid && k < 4) digests[row * 4 + k] = gl::canon(x);
 }

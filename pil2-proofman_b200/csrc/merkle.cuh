@@ -154,13 +154,13 @@ inline uint64_t tree_num_elements(uint64_t nrows, uint64_t arity)
 }
 
 // Below this many states per launch the one-thread-per-state hashing kernels leave the GPU idle
-// and take the latency of one whole permutation per thread (~40 us for W16); the cooperative
-// Poseidon2 kernels (coop.cuh, one state per 16 lanes) take it instead.
+// and take the latency of one whole permutation per thread (~40 us for Poseidon2 W16); the
+// cooperative kernels (coop.cuh, one state per 16 lanes) take it instead.
 constexpr uint64_t COOP_MAX_STATES = 8192;
 
 // Every tree level above `nrows` leaf digests already at the start of d_tree, on `stream`.
-// Poseidon2: levels of more than COOP_MAX_STATES parents one thread per parent, smaller ones
-// cooperatively, and the last levels (<= coop::TAIL_THREADS / G parents) in one launch.
+// Levels of more than COOP_MAX_STATES parents one thread per parent, smaller ones cooperatively,
+// and the last levels (<= coop::TAIL_THREADS / G parents) in one launch; both hash families.
 template <int W, int FAM = 2>
 cudaError_t build_levels(uint64_t *d_tree, uint64_t nrows, cudaStream_t stream)
 {
@@ -172,18 +172,18 @@ cudaError_t build_levels(uint64_t *d_tree, uint64_t nrows, cudaStream_t stream)
         const uint64_t pad = (ARITY - pending % ARITY) % ARITY;
         const uint64_t parents = (pending + ARITY - 1) / ARITY;
         uint64_t *lvl = d_tree + base;
-        if constexpr (FAM == 2) {
+        {
             constexpr uint64_t G = coop::Tab<W>::G;
             if (parents <= (uint64_t)coop::TAIL_THREADS / G) {
-                coop::tree_tail_kernel<W><<<1, coop::TAIL_THREADS, 0, stream>>>(lvl, pending);
+                coop::tree_tail_kernel<W, FAM><<<1, coop::TAIL_THREADS, 0, stream>>>(lvl, pending);
                 prof::count();
                 break;
             }
             if (parents <= COOP_MAX_STATES) {
                 const uint64_t threads = parents * G;
-                coop::node_coop_kernel<W><<<(unsigned)((threads + coop::CTA_THREADS - 1) / coop::CTA_THREADS),
-                                            coop::CTA_THREADS, 0, stream>>>(lvl, pending, pad, parents,
-                                                                            lvl + (pending + pad) * 4);
+                coop::node_coop_kernel<W, FAM>
+                    <<<(unsigned)((threads + coop::CTA_THREADS - 1) / coop::CTA_THREADS), coop::CTA_THREADS, 0,
+                       stream>>>(lvl, pending, pad, parents, lvl + (pending + pad) * 4);
                 prof::count();
                 base += (pending + pad) * 4;
                 pending = parents;
@@ -208,10 +208,10 @@ cudaError_t build_tree(uint64_t *d_tree, const uint64_t *d_src, uint64_t rs, uin
     const unsigned tpb = TPB;
     {
         prof::Scope ps(prof::LEAF_HASH, stream);
-        if (FAM == 2 && nrows <= COOP_MAX_STATES) {
+        if (nrows <= COOP_MAX_STATES) {
             const uint64_t threads = nrows * coop::Tab<W>::G;
-            coop::leaf_coop_kernel<W><<<(unsigned)((threads + coop::CTA_THREADS - 1) / coop::CTA_THREADS),
-                                        coop::CTA_THREADS, 0, stream>>>(d_tree, d_src, rs, cs, ncols, nrows);
+            coop::leaf_coop_kernel<W, FAM><<<(unsigned)((threads + coop::CTA_THREADS - 1) / coop::CTA_THREADS),
+                                             coop::CTA_THREADS, 0, stream>>>(d_tree, d_src, rs, cs, ncols, nrows);
         } else {
             leaf_hash_kernel<W, FAM><<<(unsigned)((nrows + tpb - 1) / tpb), tpb, 0, stream>>>(d_tree, d_src, rs, cs,
                                                                                            ncols, nrows);
