@@ -69,3 +69,17 @@ def test_product_does_not_reference_oracle():
                 text = open(os.path.join(root, f)).read()
                 assert "oracle" not in text, f
                 assert "libpil2ref" not in text and "gl_oracle" not in text, f
+
+
+def test_kernel_names_list_every_kernel(pkg):
+    """b200_kernel_names() (the launch evidence the library reports) names every __global__ kernel
+    defined in its sources, and nothing else."""
+    import glob
+    import re
+    defs = set()
+    for f in glob.glob(os.path.join(REPO, "pil2-proofman_b200", "csrc", "*.cu*")):
+        text = open(f).read()
+        for m in re.finditer(r"__global__\s+void\s+(?:__launch_bounds__\((?:[^()]|\([^()]*\))*\)\s*)?(\w+)\s*\(", text):
+            defs.add(m.group(1))
+    names = set(pkg.load().b200_kernel_names().decode().split())
+    assert defs == names, (sorted(defs - names), sorted(names - defs))
