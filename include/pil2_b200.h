@@ -118,6 +118,14 @@ void get_stream_proofs_non_blocking(void *d_buffers);
 /* starks_api.hpp:42 */
 void wait_trace_h2d_done(void *d_buffers, uint64_t stream_id);
 
+/* starks_api.hpp:40-41 (GPU backend: register_host_memory_gpu, starks_api.cu:86-104) — page-lock
+ * a caller-owned host range (whole pages) for direct DMA, as proofman's memory handler does for
+ * its trace buffers (common/src/memory_handler.rs); the trace copies of commit_witness then run at
+ * full PCIe rate.  Returns 1 when pinned, 0 otherwise (null, empty, or the driver refused);
+ * unregister ignores errors. */
+uint32_t register_host_memory(void *ptr, uint64_t size);
+void unregister_host_memory(void *ptr);
+
 /* starks_api.hpp:61 — pStarkInfo is a B200StarkShape* (nCols = nConstants).  Host const pols
  * N x nConstants row-major in, host tree out: [LDE column-major NExt*nConstants][nodes]
  * (calculate_const_tree_gpu, starks_api.cu:1932-1980).  unified_buffer_gpu, if non-NULL, is a

@@ -65,6 +65,8 @@ _SIGS = {
     "b200_fill_random_device": (_i32, [_vp, _u64, _u64, _vp]),
     "b200_fill_random_host": (None, [_vp, _u64, _u64]),
     "b200_lde_rows_device": (_i32, [_vp, _vp, _u64, _u64, _vp, _u64, _vp]),
+    "register_host_memory": (ctypes.c_uint32, [_vp, _u64]),
+    "unregister_host_memory": (None, [_vp]),
     "b200_kernel_names": (ctypes.c_char_p, []),
     "b200_timing_enable": (None, [_i32]),
     "b200_timing_reset": (None, []),

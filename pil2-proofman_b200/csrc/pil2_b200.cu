@@ -691,6 +691,21 @@ extern "C" void get_stream_proofs_non_blocking(void *d_buffers)
         if (s.busy && cudaEventQuery(s.end) == cudaSuccess) harvest(s);
 }
 
+extern "C" uint32_t register_host_memory(void *ptr, uint64_t size)
+{
+    if (!ptr || size == 0) return 0;
+    if (cudaHostRegister(ptr, size, cudaHostRegisterPortable) != cudaSuccess) {
+        cudaGetLastError();  // a refused registration leaves no sticky error
+        return 0;
+    }
+    return 1;
+}
+
+extern "C" void unregister_host_memory(void *ptr)
+{
+    if (ptr && cudaHostUnregister(ptr) != cudaSuccess) cudaGetLastError();
+}
+
 extern "C" void wait_trace_h2d_done(void *d_buffers, uint64_t stream_id)
 {
     auto *b = (CommitBuffers *)d_buffers;

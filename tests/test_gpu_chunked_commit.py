@@ -90,3 +90,33 @@ def test_poseidon1_chunked_commit_in_child_process(pkg, dev):
     assert r.returncode == 0, r.stderr[-2000:]
     res = json.loads(r.stdout.strip().splitlines()[-1])
     assert res == {"sid": 0, "err": 0, "ok": True}, res
+
+
+def test_commit_witness_from_registered_host_memory(dev, orc):
+    """proofman pins its trace buffers with register_host_memory (memory_handler.rs) before
+    committing; the commit from a registered buffer equals the oracle's, and unregistering works."""
+    import mmap
+    lib = dev.load()
+    dev.set_hash_family(2)
+    assert lib.register_host_memory(None, 4096) == 0 and lib.register_host_memory(None, 0) == 0
+    nb, nbe, nc = 16, 17, 129
+    nbytes = (1 << nb) * nc * 8
+    size = (nbytes + mmap.PAGESIZE - 1) // mmap.PAGESIZE * mmap.PAGESIZE
+    region = mmap.mmap(-1, size)  # page-aligned anonymous memory, like a Rust Vec's pages
+    trace = np.frombuffer(region, dtype=np.uint64, count=(1 << nb) * nc).reshape(1 << nb, nc)
+    trace[:] = oracle.random_field((1 << nb, nc), 777)
+    base = ctypes.addressof(ctypes.c_char.from_buffer(region))
+    assert lib.register_host_memory(base, size) == 1
+    bufs = dev.DeviceBuffers(arity=4, n_streams=2)
+    try:
+        shape = dev.StarkShape(nb, nbe, nc, 4)
+        params = dev.StepsParams()
+        params.trace = base
+        root = np.zeros(4, dtype=np.uint64)
+        assert lib.commit_witness(shape.ptr, ctypes.addressof(params), 0, 0, 0, root.ctypes.data, bufs.ptr, b"") < 2
+        lib.get_stream_proofs(bufs.ptr)
+        assert bufs.error() == 0
+        assert (root == orc.commit(np.array(trace), nbe, 4)[0]).all()
+    finally:
+        bufs.close()
+        lib.unregister_host_memory(base)
