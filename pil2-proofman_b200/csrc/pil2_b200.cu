@@ -812,12 +812,20 @@ extern "C" void calculate_const_tree(void *pStarkInfo, void *pConstPolsAddress, 
         return;
     }
     cudaStream_t s;
-    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return;
-    if (N * nCols) cudaMemcpyAsync(tr.p, pConstPolsAddress, N * nCols * 8, cudaMemcpyHostToDevice, s);
-    if (commit_device_fam(nullptr, d_tree, d_tree + NExt * nCols, tr.p, 1, sh->nBits, sh->nBitsExt, nCols,
-                           sh->arity, sc.p, s, g_hash_family.load()) == B200_OK)
-        cudaMemcpyAsync(pConstTree, d_tree, total * 8, cudaMemcpyDeviceToHost, s);
-    cudaStreamSynchronize(s);
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+        set_err(B200_ECUDA, "calculate_const_tree: stream creation failed");
+        return;
+    }
+    cudaError_t e = cudaSuccess;
+    if (N * nCols) e = cudaMemcpyAsync(tr.p, pConstPolsAddress, N * nCols * 8, cudaMemcpyHostToDevice, s);
+    int rc = e == cudaSuccess ? B200_OK : set_err(B200_ECUDA, "calculate_const_tree: trace copy failed");
+    if (!rc)
+        rc = commit_device_fam(nullptr, d_tree, d_tree + NExt * nCols, tr.p, 1, sh->nBits, sh->nBitsExt, nCols,
+                               sh->arity, sc.p, s, g_hash_family.load());
+    if (!rc && cudaMemcpyAsync(pConstTree, d_tree, total * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        rc = set_err(B200_ECUDA, "calculate_const_tree: result copy failed");
+    // the stream is drained before the device buffers are freed, whatever happened above
+    if (cudaStreamSynchronize(s) != cudaSuccess && !rc) set_err(B200_ECUDA, "calculate_const_tree: commit failed");
     cudaStreamDestroy(s);
 }
 
