@@ -6,6 +6,8 @@ at blowup 4), where the NTT runs its largest windows and the tree its deepest le
   root, every LDE word and every tree node.
 * A size-independent property for many columns: the LDE is linear, LDE(x + y) = LDE(x) + LDE(y)
   (mod p), checked word for word.
+* At the full C4 and C2 shapes (all columns): the reference-facing commit_witness path and the
+  one-pass device path give the same root.
 Calls go through the C-ABI library; torch only allocates device memory.
 """
 import numpy as np
@@ -69,3 +71,40 @@ def test_full_size_lde_is_linear(dev):
     _, ly, _ = _commit(dev, y, nbits, nbe)
     _, lz, _ = _commit(dev, z, nbits, nbe)
     assert (lz == _addmod(lx, ly)).all()
+
+
+@pytest.mark.parametrize("nbits,nbe,ncols", [(20, 22, 780), (22, 23, 256)])
+def test_full_size_commit_witness_equals_one_pass(dev, nbits, nbe, ncols):
+    """At the full C4 (2^20 x 780, blowup 4) and C2 (2^22 x 256, blowup 2) shapes, commit_witness
+    from pinned host memory (column blocks of 16, then 64, crossing PCIe while earlier blocks are
+    extended; the sponge absorbed in 12-column chunks on the idle device) gives the root of the
+    one-pass device commit (transpose, LDE, one leaf kernel).  Both are pinned to the oracle at
+    smaller sizes; here they must agree with each other on every bit of the root."""
+    import ctypes
+    pkg, torch = dev
+    N, NExt = 1 << nbits, 1 << nbe
+    d_trace = torch.empty(N * ncols, dtype=torch.int64, device="cuda")
+    pkg.fill_random_device(d_trace, N * ncols, 780 + nbits)
+    d_lde = torch.empty(NExt * ncols, dtype=torch.int64, device="cuda")
+    d_tree = torch.empty(pkg.tree_num_elements(NExt, 4), dtype=torch.int64, device="cuda")
+    d_scr = torch.empty(pkg.lde_scratch_words(nbits, ncols), dtype=torch.int64, device="cuda")
+    root_dev = pkg.commit_device(d_lde, d_tree, d_trace, nbits, nbe, ncols, 4, d_scr)
+    torch.cuda.synchronize()
+    host = torch.empty(N * ncols, dtype=torch.int64, pin_memory=True)
+    host.copy_(d_trace)
+    del d_trace, d_lde, d_tree, d_scr
+    torch.cuda.empty_cache()
+    lib = pkg.load()
+    pkg.set_hash_family(2)
+    bufs = pkg.DeviceBuffers(arity=4, n_streams=2)
+    try:
+        shape = pkg.StarkShape(nbits, nbe, ncols, 4)
+        params = pkg.StepsParams()
+        params.trace = host.data_ptr()
+        root = np.zeros(4, dtype=np.uint64)
+        assert lib.commit_witness(shape.ptr, ctypes.addressof(params), 0, 0, 0, root.ctypes.data, bufs.ptr, b"") < 2
+        lib.get_stream_proofs(bufs.ptr)
+        assert bufs.error() == 0, lib.b200_last_error()
+    finally:
+        bufs.close()
+    assert (root == root_dev).all(), (root, root_dev)
