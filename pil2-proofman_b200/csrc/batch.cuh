@@ -334,7 +334,6 @@ class Plan {
                 e.p.dst = x.scratch;
                 e.p.src_cs = N;
                 e.p.dst_cs = N;
-                e.p.ninv = glh::inv(N % GL_P);
                 e.p.lg = x.nBits;
                 e.p.s0 = w.s0;
                 e.p.k = w.k;
@@ -367,7 +366,6 @@ class Plan {
                 e.p.dst = x.lde;
                 e.p.src_cs = (j == 0) ? N : NExt;
                 e.p.dst_cs = NExt;
-                e.p.ninv = 1;
                 e.p.lg = x.nBitsExt;
                 e.p.s0 = w.s0;
                 e.p.k = w.k;

@@ -34,7 +34,7 @@ __device__ uint64_t g_ntt_tw_lo_fwd[1 << 13];
 __device__ uint64_t g_ntt_tw_hi_fwd[1 << 13];
 __device__ uint64_t g_ntt_tw_lo_inv[1 << 13];
 __device__ uint64_t g_ntt_tw_hi_inv[1 << 13];
-__device__ uint64_t g_ntt_sh_lo[1 << 12];  // 7^j
+__device__ uint64_t g_ntt_sh_lo_n[(NTT_TWLG + 1) << 12];  // 7^j * 2^-lg at [lg * 4096 + j]
 __device__ uint64_t g_ntt_sh_hi[1 << 14];  // 7^(4096 j)
 
 namespace ntt {
@@ -45,7 +45,6 @@ struct Pass {
     const uint64_t *src;
     uint64_t *dst;
     uint64_t src_cs, dst_cs;  // column strides, elements
-    uint64_t ninv;            // N^-1 for POST_COSET
     uint32_t lg;              // log2 of the transform length (dst positions)
     uint32_t s0, k, lgL;      // window: stages [s0, s0+k), 2^lgL lanes per tile
     uint32_t rep;             // source position = dst position >> rep
@@ -256,8 +255,9 @@ __device__ __forceinline__ void pass16_body(const Pass &a, uint64_t tile, uint64
         }
         if (a.post == POST_COSET) {
             const uint32_t br = brev_bits((uint32_t)pos, a.lg);
-            const uint64_t f = gl::mul(__ldg(g_ntt_sh_lo + (br & 4095)), __ldg(g_ntt_sh_hi + (br >> 12)));
-            v = gl::mul(v, gl::mul(f, a.ninv));
+            const uint64_t f =
+                gl::mul(__ldg(g_ntt_sh_lo_n + (a.lg << 12) + (br & 4095)), __ldg(g_ntt_sh_hi + (br >> 12)));
+            v = gl::mul(v, f);
         } else if (a.post == POST_CANON) {
             v = gl::canon(v);
         }
@@ -372,6 +372,38 @@ __device__ __forceinline__ void phases_fixed(uint64_t *sm)
     }
 }
 
+// Register-path tile load of a fixed-shape window: the gather (with the Q stage's source remap
+// and scale), the forward windows' inter-window twiddle, the store to shared memory.  ONE: the
+// twiddles are powers of w_8192 (s0 + K <= 13, the first forward window at blowup 2), so each is
+// one entry of the high table instead of a product of a low and a high entry.
+template <int K, int LGL, bool DIF, bool ONE>
+__device__ __forceinline__ void load_tile(uint64_t *sm, const Pass &a, const uint64_t *S, uint32_t base,
+                                          uint32_t lob, uint32_t s0, uint32_t tw_shift)
+{
+    constexpr int T = Shape<K, LGL>::T, NT = Shape<K, LGL>::NT;
+    constexpr int IT = (T + NT - 1) / NT;
+    constexpr uint32_t Lm = (1u << LGL) - 1;
+    const uint32_t rep = a.rep, gshift = a.gshift, goff = (uint32_t)a.goff;
+#pragma unroll 4  // full unrolling hoists all 16 loads of a thread and spills at 64 registers
+    for (int it = 0; it < IT; it++) {
+        const uint32_t q = threadIdx.x + (uint32_t)it * NT;
+        if ((T % NT) != 0 && q >= (uint32_t)T) break;
+        const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
+        uint64_t v = S[((pos >> rep) << gshift) + goff];
+        if (a.scale) v = gl::mul(v, a.scale);
+        if (!DIF && s0 > 0) {
+            const uint32_t lo = (lob << LGL) | (q & Lm);
+            const uint32_t E = (__brev(q >> LGL) >> (32 - K)) * lo;
+            if (ONE) {
+                if (E) v = gl::mul(v, __ldg(g_ntt_tw_hi_fwd + (E << (13 - s0 - K))));
+            } else if (E) {
+                v = gl::mul(v, big_twiddle((uint64_t)(E << tw_shift), false));
+            }
+        }
+        sm[pad16(q)] = v;
+    }
+}
+
 // One CTA of Shape<K,LGL>::NT threads: tile `tile` of column `col` of the window `a`, whose
 // direction (a.dif) is DIF.  The direction is a template parameter so that each instantiation
 // holds only its own load path and twiddle placement.
@@ -407,21 +439,10 @@ __device__ __forceinline__ void pass_fixed_body(const Pass &a, uint32_t tile, ui
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    } else if (!inv && s0 > 0 && s0 + K <= 13) {
+        load_tile<K, LGL, DIF, true>(sm, a, S, base, lob, s0, tw_shift);
     } else {
-#pragma unroll 4  // full unrolling hoists all 16 loads of a thread and spills at 64 registers
-        for (int it = 0; it < IT; it++) {
-            const uint32_t q = threadIdx.x + (uint32_t)it * NT;
-            if ((T % NT) != 0 && q >= (uint32_t)T) break;
-            const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
-            uint64_t v = S[((pos >> rep) << gshift) + goff];
-            if (a.scale) v = gl::mul(v, a.scale);
-            if (!inv && s0 > 0) {
-                const uint32_t lo = (lob << LGL) | (q & Lm);
-                const uint32_t E = (__brev(q >> LGL) >> (32 - K)) * lo;
-                if (E) v = gl::mul(v, big_twiddle((uint64_t)(E << tw_shift), false));
-            }
-            sm[pad16(q)] = v;
-        }
+        load_tile<K, LGL, DIF, false>(sm, a, S, base, lob, s0, tw_shift);
     }
     __syncthreads();
     if constexpr (inv)
@@ -441,8 +462,9 @@ __device__ __forceinline__ void pass_fixed_body(const Pass &a, uint32_t tile, ui
         }
         if (a.post == POST_COSET) {
             const uint32_t br = brev_bits(pos, a.lg);
-            const uint64_t f = gl::mul(__ldg(g_ntt_sh_lo + (br & 4095)), __ldg(g_ntt_sh_hi + (br >> 12)));
-            v = gl::mul(v, gl::mul(f, a.ninv));
+            const uint64_t f =
+                gl::mul(__ldg(g_ntt_sh_lo_n + (a.lg << 12) + (br & 4095)), __ldg(g_ntt_sh_hi + (br >> 12)));
+            v = gl::mul(v, f);
         } else if (a.post == POST_CANON) {
             v = gl::canon(v);
         }
@@ -656,7 +678,6 @@ inline cudaError_t lde(uint64_t *d_lde, const uint64_t *d_trace, bool trace_rowm
     const Tune tn = tuned(nBits, nBitsExt, ncols);
     int nw = nBits ? plan_windows(0, nBits, w, 8, tn.kfirst, tn.krest) : 0;
     if (nw < 0) return cudaErrorInvalidValue;
-    const uint64_t ninv = glh::inv(N % GL_P);
     {
     prof::Scope ps(prof::NTT_INV, stream);
     for (int i = nw - 1; i >= 0; i--) {
@@ -665,7 +686,6 @@ inline cudaError_t lde(uint64_t *d_lde, const uint64_t *d_trace, bool trace_rowm
         p.dst = d_scratch;
         p.src_cs = cur_cs;
         p.dst_cs = N;
-        p.ninv = ninv;
         p.lg = nBits;
         p.s0 = w[i].s0;
         p.k = w[i].k;
@@ -689,7 +709,6 @@ inline cudaError_t lde(uint64_t *d_lde, const uint64_t *d_trace, bool trace_rowm
         p.dst = d_lde;
         p.src_cs = (i == 0) ? cur_cs : NExt;
         p.dst_cs = NExt;
-        p.ninv = 1;
         p.lg = nBitsExt;
         p.s0 = w[i].s0;
         p.k = w[i].k;
@@ -793,7 +812,7 @@ inline cudaError_t lde_q(uint64_t *d_cmq, const uint64_t *d_q, bool q_rowmajor, 
 inline cudaError_t init_tables()
 {
     static uint64_t lo_f[1 << 13], hi_f[1 << 13], lo_i[1 << 13], hi_i[1 << 13];
-    static uint64_t sh_lo[1 << 12], sh_hi[1 << 14];
+    static uint64_t sh_lo[1 << 12], sh_hi[1 << 14], sh_lo_n[(NTT_TWLG + 1) << 12];
     static uint64_t w4096_f[4096], w4096_i[4096];
     static bool ready = false;
     if (!ready) {
@@ -810,6 +829,11 @@ inline cudaError_t init_tables()
         sh_lo[0] = sh_hi[0] = 1;
         for (int j = 1; j < (1 << 12); j++) sh_lo[j] = glh::mul(sh_lo[j - 1], 7);
         for (int j = 1; j < (1 << 14); j++) sh_hi[j] = glh::mul(sh_hi[j - 1], s4096);
+        // the coset step's 1/N folded into the low table, one copy per transform size 2^lg
+        const uint64_t half = glh::inv(2);
+        uint64_t ninv = 1;
+        for (int lg = 0; lg <= NTT_TWLG; lg++, ninv = glh::mul(ninv, half))
+            for (int j = 0; j < (1 << 12); j++) sh_lo_n[(lg << 12) + j] = glh::mul(sh_lo[j], ninv);
         const uint64_t w4096 = glh::root_of_unity(12), w4096i = glh::inv(w4096);
         w4096_f[0] = w4096_i[0] = 1;
         for (int j = 1; j < 4096; j++) {
@@ -823,7 +847,7 @@ inline cudaError_t init_tables()
     if ((e = cudaMemcpyToSymbol(g_ntt_tw_hi_fwd, hi_f, sizeof(hi_f))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(g_ntt_tw_lo_inv, lo_i, sizeof(lo_i))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(g_ntt_tw_hi_inv, hi_i, sizeof(hi_i))) != cudaSuccess) return e;
-    if ((e = cudaMemcpyToSymbol(g_ntt_sh_lo, sh_lo, sizeof(sh_lo))) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(g_ntt_sh_lo_n, sh_lo_n, sizeof(sh_lo_n))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(g_ntt_sh_hi, sh_hi, sizeof(sh_hi))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(g_ntt_w4096_fwd, w4096_f, sizeof(w4096_f))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(g_ntt_w4096_inv, w4096_i, sizeof(w4096_i))) != cudaSuccess) return e;
