@@ -200,8 +200,17 @@ __global__ void gather_roots(const uint64_t *const *tree_ends, int n, uint64_t *
 
 // ------------------------------------------------------------------ host plan ----
 
+// Instances whose window (or transpose) covers at least this many elements get the plain path's
+// own launch for it: such a launch alone fills the GPU for dozens of waves, and the plain kernel
+// reads its window description from the kernel parameters, where the grouped kernel first finds
+// its entry and stages it through shared memory (measured on B200: grouped windows 2-8 % and the
+// grouped transpose 14 % slower than the plain launches of the same instances).
+constexpr uint64_t PLAIN_MIN_ELEMS = 1ull << 27;
+
 struct Launch {
-    int kind;  // 0 transpose, 1 pass (generic), 2 leaf, 3 node, 5 pass (fixed shape width, lgl, dif)
+    // 0 transpose, 1 pass (generic), 2 leaf, 3 node, 5 pass (fixed shape width, lgl, dif),
+    // 6 one instance's window as a plain launch, 7 one instance's transpose as a plain launch
+    int kind;
     int width;
     size_t off;  // byte offset of the entry array in the device table buffer
     int n;
@@ -209,6 +218,9 @@ struct Launch {
     size_t smem;
     int lgl = 0;
     int dif = 0;
+    ntt::Pass pass{};   // kind 6
+    uint64_t ncols = 0; // kind 6
+    int inst = -1;      // kind 7
 };
 
 class Plan {
@@ -238,8 +250,19 @@ class Plan {
 
     // one window index's entries as launches: one per fixed window shape and direction, the
     // rest generic
-    void push_passes(const std::vector<PassEntry> &pe)
+    void push_passes(const std::vector<PassEntry> &all)
     {
+        std::vector<PassEntry> pe;
+        for (const PassEntry &e : all) {
+            if ((e.tiles << (e.p.k + e.p.lgL)) * e.ncols >= PLAIN_MIN_ELEMS) {
+                Launch L{6, 0, 0, 1, e.tiles * e.ncols, 0};
+                L.pass = e.p;
+                L.ncols = e.ncols;
+                launches.push_back(L);
+            } else {
+                pe.push_back(e);
+            }
+        }
         std::vector<std::array<uint32_t, 3>> shapes;
         for (const PassEntry &e : pe) {
             const std::array<uint32_t, 3> sh{e.p.k, e.p.lgL, e.p.dif ? 1u : 0u};
@@ -295,9 +318,16 @@ class Plan {
         {
             std::vector<TransposeEntry> te;
             uint64_t b = 0;
-            for (const Inst &x : inst) {
+            for (size_t i = 0; i < inst.size(); i++) {
+                const Inst &x = inst[i];
                 const uint64_t N = 1ull << x.nBits;
                 if (!x.nCols) continue;
+                if (N * x.nCols >= PLAIN_MIN_ELEMS) {
+                    Launch L{7, 0, 0, 1, 0, 0};
+                    L.inst = (int)i;
+                    launches.push_back(L);
+                    continue;
+                }
                 TransposeEntry t{x.trace, x.scratch, N, x.nCols, (N + 31) / 32, (x.nCols + 31) / 32ull, b};
                 b += t.rtiles * t.ctiles;
                 te.push_back(t);
@@ -460,6 +490,16 @@ class Plan {
             const void *ent = d_table + L.off;
             switch (L.kind) {
             case 0: transpose_grouped<<<(unsigned)L.blocks, dim3(32, 8), 0, s>>>((const TransposeEntry *)ent, L.n); break;
+            case 6:
+                if ((e = ntt::launch_pass(L.pass, L.ncols, s)) != cudaSuccess) return e;
+                continue;  // launch_pass counts its launch
+            case 7: {
+                const Inst &x = inst[(size_t)L.inst];
+                const uint64_t N = 1ull << x.nBits;
+                const dim3 grid((unsigned)((N + 31) / 32), (unsigned)((x.nCols + 31) / 32));
+                ntt::transpose_kernel<<<grid, dim3(32, 8), 0, s>>>(x.scratch, x.trace, N, x.nCols, N);
+                break;
+            }
             case 1: pass_grouped<<<(unsigned)L.blocks, 512, L.smem, s>>>((const PassEntry *)ent, L.n); break;
             case 5: {
                 const uint32_t T = 1u << (L.width + L.lgl);

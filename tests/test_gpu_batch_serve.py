@@ -86,6 +86,41 @@ def test_batch_matches_plain_and_oracle(pkg, torch_cuda, orc):
         assert (orc.commit(trace, nbe, ar)[0] == plain[j][0]).all()
 
 
+def test_batch_with_large_instances_matches_plain(pkg, torch_cuda):
+    """Instances whose windows or transpose cover >= 2^27 elements run as the plain path's own
+    launches inside the batch (the rest stay grouped); every LDE word, tree node and root must
+    still equal the plain path's, in direct runs and in graph capture and replay."""
+    torch = torch_cuda
+    pkg.init(0)
+    lib = pkg.load()
+    shapes = [(20, 21, 128, 4), (12, 13, 16, 3), (19, 21, 300, 4), (17, 18, 40, 4)]
+    bufs, descs = _alloc(torch, pkg, shapes)
+    plain = []
+    for j, (nb, nbe, nc, ar) in enumerate(shapes):
+        t = bufs[j]
+        lde, tree, scr = torch.empty_like(t["lde"]), torch.empty_like(t["tree"]), torch.empty_like(t["scratch"])
+        root = pkg.commit_device(lde, tree, t["trace"], nb, nbe, nc, ar, scr)
+        plain.append((root, lde, tree))
+        del scr
+    stream = torch.cuda.Stream()
+    plan = lib.b200_batch_plan_new(descs, len(shapes))
+    assert plan, lib.b200_last_error()
+    try:
+        for use_graph in (0, 1, 1):
+            roots = np.zeros((len(shapes), 4), dtype=np.uint64)
+            for t in bufs:
+                t["lde"].fill_(-1)
+                t["tree"].fill_(-1)
+            torch.cuda.synchronize()
+            assert lib.b200_batch_plan_run(plan, roots.ctypes.data, stream.cuda_stream, use_graph) == 0
+            for j in range(len(shapes)):
+                assert (roots[j] == plain[j][0]).all(), (j, use_graph)
+                assert torch.equal(bufs[j]["lde"], plain[j][1]), (j, use_graph)
+                assert torch.equal(bufs[j]["tree"], plain[j][2]), (j, use_graph)
+    finally:
+        lib.b200_batch_plan_free(plan)
+
+
 def test_one_shot_batch_entry(pkg, torch_cuda):
     torch = torch_cuda
     lib = pkg.load()
