@@ -520,13 +520,18 @@ extern "C" uint64_t gen_device_streams(void *d_buffers, uint64_t n_streams, uint
 // Column blocks of the pipelined commit, as start columns (starts.back() == nCols): when the
 // trace is large enough for the overlap to matter, a 16-column first block (nothing hides its
 // copy: the kernels start once it has landed; 128-byte row segments still copy at 47 GB/s), then
-// 64-column blocks (512-byte row segments, which a 2-D copy moves at the full 55 GB/s).
+// blocks of 24 and 48 columns, then 64-column blocks (512-byte row segments, which a 2-D copy
+// moves at the full 55 GB/s).  On an idle device the kernels of the blocks already landed (LDE
+// plus the chunked sponge, ~1.1 ms per 2^22-row column against ~0.6 ms of copy) must outlast the
+// next block's copy, or the GPU waits: after 16 columns that allows about 28 more, after 40
+// about 49 more.
 static void commit_blocks(uint64_t nBits, uint64_t nCols, std::vector<uint64_t> &starts)
 {
     starts.assign(1, 0);
     if (nBits >= 16 && nCols >= 128) {
         starts.push_back(16);
-        for (uint64_t c = 64; c < nCols; c += 64) starts.push_back(c);
+        starts.push_back(40);
+        for (uint64_t c = 88; c < nCols; c += 64) starts.push_back(c);
     }
     if (nCols) starts.push_back(nCols);
 }
