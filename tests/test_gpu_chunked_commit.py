@@ -3,7 +3,8 @@ are still crossing PCIe; with an earlier commit in flight it uses the one-pass l
 
 Both orders must give the reference root (oracle: NTT_Goldilocks::LDE + the row sponge and
 arity-4 tree, poseidon2_goldilocks.cpp:42-175).  Shapes are large enough (N >= 2^16, >= 128
-columns) for the trace to cross in several 64-column blocks, with ragged last blocks and chunks.
+columns) for the trace to cross in several column blocks (16, 24, 48, then 64 columns), with ragged
+last blocks and chunks.
 Poseidon1 runs in a child process because set_hash_family is once per process.
 """
 import ctypes
