@@ -76,9 +76,9 @@ def test_full_size_lde_is_linear(dev):
 @pytest.mark.parametrize("nbits,nbe,ncols", [(20, 22, 780), (22, 23, 256)])
 def test_full_size_commit_witness_equals_one_pass(dev, nbits, nbe, ncols):
     """At the full C4 (2^20 x 780, blowup 4) and C2 (2^22 x 256, blowup 2) shapes, commit_witness
-    from pinned host memory (column blocks of 16, 24, 48, then 64, crossing PCIe while earlier blocks are
-    extended; the sponge absorbed in 12-column chunks on the idle device) gives the root of the
-    one-pass device commit (transpose, LDE, one leaf kernel).  Both are pinned to the oracle at
+    from pinned host memory (column blocks of 16, 24, 48, then 64, crossing PCIe while earlier
+    blocks are extended; the sponge absorbed in 12-column chunks on the idle device) gives the root
+    of the one-pass device commit (transpose, LDE, one leaf kernel).  Both are pinned to the oracle at
     smaller sizes; here they must agree with each other on every bit of the root."""
     import ctypes
     pkg, torch = dev
