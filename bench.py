@@ -15,7 +15,9 @@ HBM -> column-major LDE -> leaf digests -> every tree level -> root read back to
 
 --impl reference times the reference's own CPU implementation (NTT_Goldilocks::LDE +
 Poseidon2Goldilocks<16>::merkletree, compiled unmodified under oracle/_ref) with every host
-thread, on a bounded row sample of the same workload, in the same unit.
+thread, on the same full workload and the same seeded trace, in the same unit; that process loads
+only the reference build.  Every arm checks its root against the reference CPU root of that trace
+recorded in tests/golden/full_size.json.
 """
 import argparse
 import ctypes
@@ -33,16 +35,16 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 
 WORKLOADS = {
     "c2": dict(desc="single AIR 2^22 x 256 base columns, blowup 2, Poseidon2 W16 arity-4 tree",
-               nbits=22, nbits_ext=23, ncols=256, arity=4, sample_nbits=17),
+               nbits=22, nbits_ext=23, ncols=256, arity=4),
     "c1": dict(desc="single AIR 2^16 x 32 base columns, blowup 2, Poseidon2 W16 arity-4 tree",
-               nbits=16, nbits_ext=17, ncols=32, arity=4, sample_nbits=16),
+               nbits=16, nbits_ext=17, ncols=32, arity=4),
     # stage-2-style commit: 600 base + 60 cubic-extension columns (3 limbs each, hashed in row-major
     # limb order) = 780 words per row, blowup 4 (LDE 2^22 rows, 26 GB)
     "c4": dict(desc="stage-2 AIR 2^20 x (600 base + 60 cubic = 780 limbs), blowup 4, Poseidon2 W16 arity-4 tree",
-               nbits=20, nbits_ext=22, ncols=780, arity=4, sample_nbits=14),
+               nbits=20, nbits_ext=22, ncols=780, arity=4),
     # profiling case of the 256-column workload: LDE 2.1 GB (larger than L2), ~4.3 GB on the device
     "c2s": dict(desc="single AIR 2^19 x 256 base columns, blowup 2, Poseidon2 W16 arity-4 tree",
-                nbits=19, nbits_ext=20, ncols=256, arity=4, sample_nbits=16),
+                nbits=19, nbits_ext=20, ncols=256, arity=4),
 }
 METRIC = "LDE+Merkle commit GElem/s (NExt x nCols per second), bit-exact roots"
 UNIT = "GElem/s"
@@ -154,50 +156,108 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def host_ram_gb():
+    try:
+        return os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 1e9
+    except (ValueError, OSError, AttributeError):
+        return 0.0
+
+
+TRACE_SEED = 1000  # seed of the benchmarked trace on every rank (tests/golden/full_size.json pins its root)
+
+
+def full_size_fixture(wl):
+    """The reference CPU build's root for this workload's seeded trace, if make_full_size.py recorded it."""
+    path = os.path.join(REPO, "tests", "golden", "full_size.json")
+    try:
+        with open(path) as f:
+            for s in json.load(f)["shapes"]:
+                if (s["nBits"], s["nBitsExt"], s["nCols"], s["arity"], s["seed"]) == (
+                        wl["nbits"], wl["nbits_ext"], wl["ncols"], wl["arity"], TRACE_SEED):
+                    return s
+    except (OSError, KeyError, ValueError):
+        pass
+    return None
+
+
+def bench_config(args, wl, world):
+    """The config object both arms print (identical, so the two lines describe the same workload)."""
+    nbits, nbe, ncols, arity = wl["nbits"], wl["nbits_ext"], wl["ncols"], wl["arity"]
+    return {"workload": wl["desc"], "nBits": nbits, "nBitsExt": nbe, "nCols": ncols, "arity": arity,
+            "hash": "%s W%d" % (HASH_NAME[args.hash_family], 4 * arity),
+            "parallelism": "instance per GPU" if world > 1 else "single GPU",
+            "trace_seed": TRACE_SEED,
+            "l2": ("inputs (%.1f GB) larger than L2; no flush" if (1 << nbits) * ncols * 8 > 126e6 else
+                   "inputs (%.3f GB) fit in L2; no flush") % ((1 << nbits) * ncols * 8 / 1e9)}
+
+
 def time_reference_cpu(wl, reps, warmup, family=2):
-    """Reference CPU LDE + tree on a row sample; returns (GElem/s, seconds per rep, threads, sample)."""
+    """The reference's CPU commit (NTT_Goldilocks::LDE + merkletree, compiled unmodified under oracle/_ref)
+    of the full workload shape, with every host thread, as commit_witness_cpu runs it
+    (starks_api.cpp:683-721: LDE into the extended buffer with a caller work buffer, then the tree).
+    The trace is the benchmarked one (seeded rule of ref_fill_random == the product's generator), so the
+    root is the one the GPU arm must produce.  Returns (GElem/s, seconds per rep, threads, sample, root)."""
     sys.path.insert(0, REPO)
-    import oracle  # CPU baseline leg only
+    import oracle  # CPU baseline / reference legs only
 
     threads = cpu_threads()
     ref = oracle.RefCPU(threads=threads, family=family)
-    nb = wl["sample_nbits"]
-    b = wl["nbits_ext"] - wl["nbits"]
+    nb, nbe = wl["nbits"], wl["nbits_ext"]
     ncols, arity = wl["ncols"], wl["arity"]
-    pkg = load_package()
-    trace = pkg.fill_random_host((1 << nb) * ncols, 7).reshape(1 << nb, ncols)
-    lde = np.empty((1 << (nb + b), ncols), dtype=np.uint64)
-    tree = np.empty(oracle.tree_num_elements(1 << (nb + b), arity), dtype=np.uint64)
+    N, NExt = 1 << nb, 1 << nbe
+    # the reference's LDE work buffer is NExt x ncols (nblock 1); on a host with less memory than the
+    # trace, LDE, buffer and tree need, the buffer is split over column blocks (same values)
+    need_gb = (N + 2 * NExt) * ncols * 8 / 1e9
+    nblock = 1 if host_ram_gb() > 1.6 * need_gb else 4
+    trace = ref.fill_random(N * ncols, TRACE_SEED).reshape(N, ncols)
+    lde = np.empty((NExt, ncols), dtype=np.uint64)
+    buf = np.empty(NExt * -(-ncols // nblock), dtype=np.uint64)
+    tree = np.empty(oracle.tree_num_elements(NExt, arity), dtype=np.uint64)
     times = []
     for i in range(warmup + reps):
         t0 = time.perf_counter()
-        ref.lde_raw(trace, nb + b, out=lde)
+        ref.lde_raw(trace, nbe, out=lde, buffer=buf, nblock=nblock)
         ref.merkletree_raw(lde, arity, tree=tree)
         t1 = time.perf_counter()
         if i >= warmup:
             times.append(t1 - t0)
-    sec = statistics.median(times)
-    elems = (1 << (nb + b)) * ncols
-    sample = "%d x %d trace -> %d x %d LDE + %s W%d arity-%d tree (1/%d of the rows), %s build" % (
-        1 << nb, ncols, 1 << (nb + b), ncols, HASH_NAME[family], 4 * arity, arity, 1 << (wl["nbits"] - nb),
-        ref.variant)
-    return elems / sec / 1e9, sec, threads, sample
+    root = oracle.RefCPU.canon(tree[-4:])
+    sec = sum(times) / len(times)
+    sample = ("full workload: %d x %d trace -> %d x %d LDE + %s W%d arity-%d tree, %s build, %d warm-up + %d "
+              "timed commits, LDE work buffer in %d column block(s), %s" % (
+                  N, ncols, NExt, ncols, HASH_NAME[family], 4 * arity, arity, ref.variant, warmup, reps, nblock,
+                  cpu_model()))
+    return NExt * ncols / sec / 1e9, sec, threads, sample, root
 
 
 def run_reference(args, wl):
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    val, sec, threads, sample = time_reference_cpu(wl, args.steps, args.warmup, args.hash_family)
+    val, sec, threads, sample, root = time_reference_cpu(wl, args.steps, args.warmup, args.hash_family)
+    fx = full_size_fixture(wl) if args.hash_family == 2 else None
     line = {
         "impl": "reference", "metric": METRIC, "value": round(val, 6), "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": wl["desc"], "nBits": wl["nbits"], "nBitsExt": wl["nbits_ext"], "nCols": wl["ncols"],
-                   "arity": wl["arity"], "sample_rows": 1 << wl["sample_nbits"]},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded uniform Goldilocks)",
+        "config": bench_config(args, wl, args.gpus),
         "cpu_baseline": {"value": round(val, 6), "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": round(val, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "root": [hex(int(v)) for v in root],
+        "root_matches_fixture": None if fx is None else [int(v) for v in root] == fx["root"],
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -240,7 +300,7 @@ def run_ours(args, wl):
     scratch = torch.empty(pkg.lde_scratch_words(nbits, ncols), dtype=torch.int64, device=dev)
     lde = torch.empty(elems, dtype=torch.int64, device=dev)
     tree = torch.empty(pkg.tree_num_elements(NExt, arity), dtype=torch.int64, device=dev)
-    pkg.fill_random_device(trace, N * ncols, 1000 + rank, stream)
+    pkg.fill_random_device(trace, N * ncols, TRACE_SEED, stream)
     tuned = None
     if args.autotune:  # untimed set-up: pick the NTT window plan for this shape
         t_ms, kf, kr = pkg.autotune_lde(nbits, nbe, ncols)
@@ -365,13 +425,15 @@ def finish(args, wl, pkg, dist, rank, world, value, ms, launches, kernel_ms, roo
     nbits, nbe, ncols, arity = wl["nbits"], wl["nbits_ext"], wl["ncols"], wl["arity"]
     N = 1 << nbits
     w = 4 * arity
+    fx = full_size_fixture(wl) if args.hash_family == 2 else None
+    if fx is not None and [int(v) for v in roots[0]] != fx["root"]:
+        raise RuntimeError("root %s differs from the reference CPU root %s of the same trace (full_size.json)"
+                           % ([hex(int(v)) for v in roots[0]], [hex(v) for v in fx["root"]]))
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform Goldilocks)",
-        "config": {"workload": wl["desc"], "nBits": nbits, "nBitsExt": nbe, "nCols": ncols, "arity": arity,
-                   "hash": "%s W%d" % (HASH_NAME[args.hash_family], w), "parallelism": "instance per GPU" if world > 1 else "single GPU",
-                   "l2": "inputs (%.1f GB) larger than L2; no flush" % (N * ncols * 8 / 1e9)},
+        "config": bench_config(args, wl, world),
         "e2e": e2e_obj,
         "gpu_launches": int(launches),
         "kernel_ms_per_step": kernel_ms,
@@ -379,11 +441,15 @@ def finish(args, wl, pkg, dist, rank, world, value, ms, launches, kernel_ms, roo
         "roofline": roofline,
         "clocks": clocks,
         "root": [hex(int(v)) for v in roots[0]] if rank == 0 else None,
+        "root_check": ("equal to the reference CPU build's root of the same seeded trace "
+                       "(tests/golden/full_size.json)" if fx is not None else "no reference fixture for this shape"),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        val, sec, threads, sample = time_reference_cpu(wl, 1, 0, args.hash_family)
+        val, sec, threads, sample, cpu_root = time_reference_cpu(wl, 1, 1, args.hash_family)
         line["cpu_baseline"] = {"value": round(val, 6), "unit": UNIT, "cores": threads, "kind": "reference",
-                                "sample": sample}
+                                "sample": sample, "root_equal": bool((cpu_root == roots[0]).all())}
+        if not (cpu_root == roots[0]).all():
+            raise RuntimeError("the reference CPU root of the benchmarked trace differs from the GPU root")
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

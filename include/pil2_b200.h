@@ -75,8 +75,9 @@ typedef struct B200StepsParams {
     uint64_t *pCustomCommitsFixed;
 } B200StepsParams;
 
-/* starks_api.hpp:28 — 1 = Poseidon1 (not provided: later commits fail with B200_EFAMILY),
- * 2 = Poseidon2.  Must be called before the reference-ABI commit entries. */
+/* starks_api.hpp:28 — 1 = Poseidon1 (PoseidonGoldilocks<W>), 2 = Poseidon2 (Poseidon2Goldilocks<W>);
+ * the reference-ABI commit entries hash with the family set here.  Must be called before them,
+ * once per process (a different second value is refused, as in the reference). */
 void set_hash_family(uint8_t fam);
 
 /* starks_api.hpp:52 — per-device set-up (twiddle/coset tables, kernel attributes) for the

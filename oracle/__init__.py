@@ -31,12 +31,25 @@ def _ptr(a):
     return a.ctypes.data_as(_vp)
 
 
+def reference_root():
+    """The reference checkout: $PIL2_PROOFMAN_REF, else a directory `reference` beside this
+    repository; None when neither holds pil2-stark (e.g. on a host that only runs prebuilt files)."""
+    for cand in (os.environ.get("PIL2_PROOFMAN_REF"), os.path.join(os.path.dirname(os.path.dirname(HERE)),
+                                                                   "reference")):
+        if cand and os.path.isdir(os.path.join(cand, "pil2-stark")):
+            return cand
+    return None
+
+
 def build(ref=True):
     """Compile the restatement (and, where the reference tree is present, _ref)."""
     targets = ["oracle"]
-    if ref and os.path.isdir("/root/reference/pil2-stark"):
+    extra = []
+    root = reference_root()
+    if ref and root:
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+        extra.append("REF=" + root)
+    subprocess.run(["make", "-s", "-C", HERE] + targets + extra, check=True)
 
 
 def tree_num_elements(nrows, arity):
@@ -252,6 +265,9 @@ class RefCPU(_Base):
         lib.ref_p1_linear_hash.argtypes = [_u64, _vp, _vp, _u64]
         lib.ref_p1_merkletree.argtypes = [_u64, _vp, _vp, _u64, _u64, _u64]
         lib.ref_p1_merkletree.restype = ctypes.c_int
+        lib.ref_commit_q.argtypes = [_vp, _vp, _vp, _vp, _u64, _u64, _u64, _u64, _u64]
+        lib.ref_commit_q.restype = ctypes.c_int
+        lib.ref_fill_random.argtypes = [_vp, _u64, _u64]
         self.lib = lib
         self.variant = variant
         if threads:
@@ -304,19 +320,48 @@ class RefCPU(_Base):
         self.lib.ref_ntt(_ptr(out), _ptr(mat), mat.shape[0], mat.shape[1], 1 if inverse else 0)
         return self.canon(out)
 
-    def lde_raw(self, trace, nbits_ext, out=None):
-        """Uncanonicalised LDE into a caller buffer (timing path)."""
+    def lde_raw(self, trace, nbits_ext, out=None, buffer=None, nblock=1):
+        """Uncanonicalised LDE into a caller buffer (timing path).  ``buffer`` (optional) is the
+        NTT's work area of NExt x ceil(ncols / nblock) words; without it the reference allocates
+        NExt x ncols words itself."""
         n, ncols = trace.shape
         if out is None:
             out = np.empty((1 << nbits_ext, ncols), dtype=np.uint64)
-        self.lib.ref_lde(_ptr(out), _ptr(trace), n, 1 << nbits_ext, ncols, None, 1)
+        if buffer is not None:
+            assert buffer.size >= (1 << nbits_ext) * -(-ncols // nblock)
+        self.lib.ref_lde(_ptr(out), _ptr(trace), n, 1 << nbits_ext, ncols, _ptr(buffer),
+                         nblock if buffer is not None else 1)
+        return out
+
+    def commit_q(self, q, nbits, nbits_ext, qdeg, qdim, arity):
+        """Starks::computeQ on the reference's NTT: q row-major (NExt, qDim) -> (root, cmQ
+        row-major (NExt, qDeg*qDim), tree), all canonical."""
+        q = np.ascontiguousarray(q, dtype=np.uint64)
+        next_ = 1 << nbits_ext
+        root = np.zeros(4, dtype=np.uint64)
+        cmq = np.zeros((next_, qdeg * qdim), dtype=np.uint64)
+        tree = np.zeros(tree_num_elements(next_, arity), dtype=np.uint64)
+        if self.lib.ref_commit_q(_ptr(root), _ptr(cmq), _ptr(tree), _ptr(q), nbits, nbits_ext, qdeg, qdim, arity):
+            raise ValueError("bad Q shape")
+        return self.canon(root), self.canon(cmq), self.canon(tree)
+
+    def fill_random(self, n, seed):
+        """n seeded field elements, the same rule as the product's fill_random (splitmix64 keyed by
+        (seed, index), rejection below p), filled with every OpenMP thread."""
+        out = np.empty(n, dtype=np.uint64)
+        self.lib.ref_fill_random(_ptr(out), n, seed)
         return out
 
     def merkletree_raw(self, matrix, arity, tree=None):
+        """Uncanonicalised tree of a row-major matrix into a caller buffer (timing path), with the
+        family this checker was created for."""
         nrows, ncols = matrix.shape
         if tree is None:
             tree = np.empty(tree_num_elements(nrows, arity), dtype=np.uint64)
-        self.lib.ref_merkletree(_ptr(tree), _ptr(matrix), ncols, nrows, arity)
+        if self.family == 1:
+            self.lib.ref_p1_merkletree(0, _ptr(tree), _ptr(matrix), ncols, nrows, arity)
+        else:
+            self.lib.ref_merkletree(_ptr(tree), _ptr(matrix), ncols, nrows, arity)
         return tree
 
 

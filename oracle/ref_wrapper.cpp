@@ -120,6 +120,67 @@ int ref_commit(uint64_t *root, uint64_t *lde, uint64_t *tree, const uint64_t *tr
     return 0;
 }
 
+// Starks::computeQ (pil2-stark/src/starkpil/starks.hpp:186-239) on the reference's NTT and field
+// code: q (row-major NExt x qDim evaluations) -> INTT over NExt -> chunk p of N coefficients times
+// S[p] = (shift^-1)^(N*p) into cmQ[(i*qDeg + p)*qDim + k] -> zero rows N..NExt -> NTT over NExt ->
+// Poseidon2 tree.  The reference multiplies each chunk as a cubic-extension element by the base
+// scalar S[p] (Goldilocks3::mul), i.e. limb by limb, which is what the loop below does for any qDim.
+// cmq: NExt x (qDeg*qDim) row-major, tree: ref_tree_num_elements(NExt, arity) words.
+int ref_commit_q(uint64_t *root, uint64_t *cmq, uint64_t *tree, const uint64_t *q, uint64_t nBits, uint64_t nBitsExt,
+                 uint64_t qDeg, uint64_t qDim, uint64_t arity)
+{
+    const uint64_t N = 1ULL << nBits, NExt = 1ULL << nBitsExt, ncols = qDeg * qDim;
+    if (nBitsExt < nBits || qDeg == 0 || qDim == 0 || qDeg * N > NExt) return -1;
+    std::vector<GE> coef(NExt * qDim);
+    std::memcpy(coef.data(), q, NExt * qDim * 8);
+    NTT_Goldilocks nttExtended(NExt);
+    nttExtended.INTT(coef.data(), coef.data(), NExt, qDim);
+    std::vector<GE> S(qDeg);
+    const GE shiftIn = Goldilocks::exp(Goldilocks::inv(Goldilocks::shift()), N);
+    S[0] = Goldilocks::one();
+    for (uint64_t p = 1; p < qDeg; p++) S[p] = Goldilocks::mul(S[p - 1], shiftIn);
+    GE *cm = (GE *)cmq;
+#pragma omp parallel for collapse(2)
+    for (uint64_t p = 0; p < qDeg; p++)
+        for (uint64_t i = 0; i < N; i++)
+            for (uint64_t k = 0; k < qDim; k++)
+                cm[(i * qDeg + p) * qDim + k] = Goldilocks::mul(coef[(p * N + i) * qDim + k], S[p]);
+#pragma omp parallel for
+    for (uint64_t i = N * ncols; i < NExt * ncols; i++) cm[i] = Goldilocks::zero();
+    nttExtended.NTT(cm, cm, NExt, ncols);
+    int rc = ref_merkletree(tree, cmq, ncols, NExt, arity);
+    if (rc) return rc;
+    const uint64_t n = getTreeNumElements(NExt, (uint32_t)arity);
+    for (int i = 0; i < 4; i++) root[i] = Goldilocks::toU64(((GE *)tree)[n - 4 + i]);
+    return 0;
+}
+
+// Seeded test data: element i of stream `seed` is the first splitmix64 output below p keyed by
+// (seed, i, j), j = 0, 1, ...  The same rule as the product's b200_fill_random_host/_device, so
+// a device-filled trace and a trace filled here are identical without either side loading the
+// other's library.
+static inline uint64_t fill_mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+void ref_fill_random(uint64_t *buf, uint64_t n, uint64_t seed)
+{
+    const uint64_t key0 = fill_mix64(seed * 0x9e3779b97f4a7c15ULL + 0x632be59bd9b4e019ULL);
+#pragma omp parallel for schedule(static)
+    for (uint64_t i = 0; i < n; i++) {
+        const uint64_t key = key0 ^ (i * 0x9e3779b97f4a7c15ULL);
+        uint64_t v;
+        for (uint64_t j = 0;; j++) {
+            v = fill_mix64(key + j * 0xd1b54a32d192ed03ULL);
+            if (v < 0xFFFFFFFF00000001ULL) break;
+        }
+        buf[i] = v;
+    }
+}
+
 // Canonicalise a buffer in place (x mod p), the form every comparison uses.
 void ref_canonicalize(uint64_t *buf, uint64_t n)
 {

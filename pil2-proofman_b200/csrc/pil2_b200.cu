@@ -279,8 +279,7 @@ extern "C" const char *b200_kernel_names(void)
 {
     return "pass16_kernel\ntranspose_kernel\nleaf_hash_kernel\nnode_kernel\npermute_kernel\nlde_rows_kernel\n"
            "fill_kernel\nimad_probe_kernel\ntranspose_grouped\npass_grouped\nleaf_persistent\n"
-           "node_grouped\ngather_roots\npass_fixed_kernel\nopenings_kernel\nunpack_kernel\nunpack_indexed_kernel\n"
-           "unpack_indexed_param_kernel\n"
+           "node_grouped\ngather_roots\npass_fixed_kernel\nopenings_kernel\nbitfield_unpack_kernel\n"
            "unpack_range_kernel\nabsorb_kernel\npass_fixed_grouped\nnode_coop_kernel\ntree_tail_kernel\n"
            "leaf_coop_kernel\n";
 }
@@ -1117,11 +1116,11 @@ extern "C" int b200_commit_packed_device(uint64_t *root_host, uint64_t *d_lde, u
         for (uint64_t c = 0; c < nCols; c++) cols.v[c] = (uint8_t)col_bits[c];
         {
             prof::Scope ps(prof::TRANSPOSE, s);
-            unpack::unpack_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(d_scratch, d_packed, N, nCols,
-                                                                             words_per_row, cols);
+            CK(unpack::launch(d_scratch, d_packed, (const uint64_t *)nullptr, N, words_per_row, 0, 0, 0, cols, 0,
+                              (uint32_t)nCols, s),
+               "unpack");
             prof::count();
         }
-        CK(cudaGetLastError(), "unpack");
         // the trace now sits column-major in the scratch; the LDE transforms it in place
         CK(ntt::lde(d_lde, d_scratch, false, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, d_scratch, s), "lde");
     }
@@ -1411,12 +1410,11 @@ extern "C" int b200_commit_indexed_device(uint64_t *root_host, uint64_t *d_lde, 
         for (uint64_t c = 0; c < nCols; c++) cols.v[c] = (uint8_t)((info[c] & 127) | ((info[c] >> 32) << 7));
         {
             prof::Scope ps(prof::TRANSPOSE, s);
-            unpack::unpack_indexed_param_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(
-                d_scratch, d_rows, d_table, N, words_per_row, words_per_entry, num_entries, index_bits, cols, 0,
-                (uint32_t)nCols);
+            CK(unpack::launch(d_scratch, d_rows, d_table, N, words_per_row, words_per_entry, num_entries,
+                              (uint32_t)index_bits, cols, 0, (uint32_t)nCols, s),
+               "indexed unpack");
             prof::count();
         }
-        CK(cudaGetLastError(), "indexed unpack");
         CK(ntt::lde(d_lde, d_scratch, false, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, d_scratch, s), "lde");
     }
     CK(merkle::build_tree_arity(arity, d_tree, d_lde, 1, NExt, nCols, NExt, s, g_native_family.load()), "merkletree");

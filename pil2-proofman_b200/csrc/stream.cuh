@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(merkle::TPB, merkle::Family<FAM>::MIN_CTAS) ab
 }
 
 // Indexed witness: the instruction table on the device and the row header width; the slot's
-// width region then holds width | source << 32 per column (unpack::unpack_indexed_kernel).
+// width region then holds width | source << 32 per column (unpack::bitfield_unpack_kernel).
 struct Indexed {
     const uint64_t *table;
     uint64_t num_entries, words_per_entry, index_bits;
@@ -102,14 +102,15 @@ inline cudaError_t run(uint64_t *slot, const Layout &l, uint64_t nBits, uint64_t
     cudaError_t e;
     for (uint64_t c0 = 0; c0 < nCols; c0 += RATE) {
         const uint32_t cc = (uint32_t)((nCols - c0) < RATE ? (nCols - c0) : RATE);
-        if (ix)
-            unpack::unpack_indexed_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(
-                scr, slot + l.packed, ix->table, N, wordsPerRow, ix->words_per_entry, ix->num_entries, ix->index_bits,
-                slot + l.widths, (uint32_t)c0, cc);
-        else
+        if (ix) {
+            e = unpack::launch(scr, slot + l.packed, ix->table, N, wordsPerRow, ix->words_per_entry, ix->num_entries,
+                               (uint32_t)ix->index_bits, unpack::InfoDev{slot + l.widths}, (uint32_t)c0, cc, s);
+            if (e != cudaSuccess) return e;
+        } else {
             unpack_range_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(scr, slot + l.packed, slot + l.widths,
                                                                            slot + l.offsets, N, wordsPerRow,
                                                                            (uint32_t)c0, cc);
+        }
         prof::count();
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         if ((e = ntt::lde(chunk, scr, false, (uint32_t)nBits, (uint32_t)nBitsExt, cc, scr, s)) != cudaSuccess) return e;

@@ -16,9 +16,13 @@ Two sources, both from the reference (run here, where it is mounted):
      rows, W8 permute of 0..7 (plonky3 cross-check), W16 permute of 0..15).
 2. Outputs of the reference CPU implementation itself (NTT_Goldilocks::LDE and
    Poseidon2Goldilocks<W>::merkletree, compiled unmodified by oracle/Makefile) on
-   seeded inputs: Merkle roots and an LDE digest per shape.
+   seeded inputs: Merkle roots and an LDE digest per shape; and the Q-stage commit
+   (Starks::computeQ, starks.hpp:186-239: NTT_Goldilocks::INTT over NExt, the chunk scaling by
+   (shift^-1)^(N*p), NTT_Goldilocks::NTT, Poseidon2 tree) as ref_commit_q in
+   oracle/ref_wrapper.cpp runs it on the reference's NTT and field code.
 
-Usage (needs /root/reference and `make -C oracle ref`):  python tests/golden/make_golden.py
+Usage (needs the reference checkout, found as oracle.reference_root() finds it, and
+`make -C oracle ref`):  python tests/golden/make_golden.py
 """
 import hashlib
 import json
@@ -33,7 +37,7 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 import oracle  # noqa: E402
 
-REF = "/root/reference/pil2-stark/src/goldilocks/tests"
+REF = os.path.join(oracle.reference_root() or "reference", "pil2-stark", "src", "goldilocks", "tests")
 
 # seeded shapes pinned by the reference CPU path: (nBits, nBitsExt, ncols, arity, seed).
 # NExt = 4 is left out: there NTT_Goldilocks::NTT_iters clamps nphase to 2 (ntt_goldilocks.cpp:67-72),
@@ -68,6 +72,19 @@ SEEDED_P1 = [
     (8, 9, 7, 2, 23),
     (10, 11, 32, 4, 24),
     (12, 14, 12, 4, 25),
+]
+
+
+# seeded Q-stage commits: (nBits, nBitsExt, qDeg, qDim, arity, seed); qDim 3 is the cubic extension
+# the reference's computeQ assumes (FIELD_EXTENSION), qDeg up to NExt / N
+SEEDED_Q = [
+    (4, 6, 3, 3, 4, 41),
+    (6, 7, 2, 3, 4, 42),
+    (8, 10, 4, 3, 3, 43),
+    (10, 11, 1, 3, 2, 44),
+    (5, 9, 16, 3, 4, 45),
+    (12, 14, 3, 3, 4, 46),
+    (14, 15, 2, 3, 4, 47),
 ]
 
 
@@ -141,6 +158,15 @@ def main():
                         "root": [int(v) for v in root], "tree_sha256": digest(tree)})
         print("seeded poseidon1", nbits, nbits_ext, ncols, arity, [hex(int(v)) for v in root])
     kats["seeded_commits_poseidon1"] = seeded1
+    seeded_q = []
+    for nbits, nbits_ext, qdeg, qdim, arity, seed in SEEDED_Q:
+        q = oracle.random_field((1 << nbits_ext, qdim), seed)
+        root, cmq, tree = ref.commit_q(q, nbits, nbits_ext, qdeg, qdim, arity)
+        seeded_q.append({"nBits": nbits, "nBitsExt": nbits_ext, "qDeg": qdeg, "qDim": qdim, "arity": arity,
+                         "seed": seed, "root": [int(v) for v in root], "cmq_sha256": digest(cmq),
+                         "tree_sha256": digest(tree), "cmq_row1": [int(v) for v in cmq[1]]})
+        print("seeded Q", nbits, nbits_ext, qdeg, qdim, arity, [hex(int(v)) for v in root])
+    kats["seeded_q_commits"] = seeded_q
     kats["seeded_generator"] = "oracle.random_field: numpy PCG64(seed), uniform u64 rejected unless < p, row-major"
     with open(os.path.join(HERE, "reference_kats.json"), "w") as f:
         json.dump(kats, f, indent=1)

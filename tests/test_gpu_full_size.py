@@ -6,10 +6,16 @@ at blowup 4), where the NTT runs its largest windows and the tree its deepest le
   root, every LDE word and every tree node.
 * A size-independent property for many columns: the LDE is linear, LDE(x + y) = LDE(x) + LDE(y)
   (mod p), checked word for word.
-* At the full C4 and C2 shapes (all columns): the reference-facing commit_witness path and the
-  one-pass device path give the same root.
+* At the full C2 (2^22 x 256, blowup 2) and C4 (2^20 x 780, blowup 4) shapes, every column:
+  the one-pass device commit and the reference-facing commit_witness path against the reference's
+  own CPU build run on the same seeded trace (tests/golden/full_size.json, written by
+  make_full_size.py): root, the SHA-256 of the whole tree buffer, and sampled LDE rows.
 Calls go through the C-ABI library; torch only allocates device memory.
 """
+import hashlib
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -73,32 +79,55 @@ def test_full_size_lde_is_linear(dev):
     assert (lz == _addmod(lx, ly)).all()
 
 
-@pytest.mark.parametrize("nbits,nbe,ncols", [(20, 22, 780), (22, 23, 256)])
-def test_full_size_commit_witness_equals_one_pass(dev, nbits, nbe, ncols):
-    """At the full C4 (2^20 x 780, blowup 4) and C2 (2^22 x 256, blowup 2) shapes, commit_witness
-    from pinned host memory (column blocks of 16, 24, 48, then 64, crossing PCIe while earlier
-    blocks are extended; the sponge absorbed in 12-column chunks on the idle device) gives the root
-    of the one-pass device commit (transpose, LDE, one leaf kernel).  Both are pinned to the oracle at
-    smaller sizes; here they must agree with each other on every bit of the root."""
+def _full_size_fixtures():
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "full_size.json")
+    with open(path) as f:
+        return json.load(f)["shapes"]
+
+
+def _sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<u8").tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("fx", _full_size_fixtures(), ids=lambda fx: fx["name"])
+def test_full_size_matches_reference_cpu(dev, fx):
+    """The full workload shapes, every column, against the reference CPU build's commit of the same
+    seeded trace (NTT_Goldilocks::LDE + Poseidon2Goldilocks<16>::merkletree, run by
+    make_full_size.py): the one-pass device commit (root, the whole tree buffer by SHA-256, sampled
+    LDE rows word for word), then commit_witness from pinned host memory (column blocks of 16, 24,
+    48, then 64, crossing PCIe while earlier blocks are extended; the sponge absorbed in 12-column
+    chunks on the idle device) to the same root."""
     import ctypes
     pkg, torch = dev
+    nbits, nbe, ncols, arity = fx["nBits"], fx["nBitsExt"], fx["nCols"], fx["arity"]
     N, NExt = 1 << nbits, 1 << nbe
+    want_root = np.array(fx["root"], dtype=np.uint64)
     d_trace = torch.empty(N * ncols, dtype=torch.int64, device="cuda")
-    pkg.fill_random_device(d_trace, N * ncols, 780 + nbits)
+    pkg.fill_random_device(d_trace, N * ncols, fx["seed"])
     d_lde = torch.empty(NExt * ncols, dtype=torch.int64, device="cuda")
-    d_tree = torch.empty(pkg.tree_num_elements(NExt, 4), dtype=torch.int64, device="cuda")
+    d_tree = torch.empty(pkg.tree_num_elements(NExt, arity), dtype=torch.int64, device="cuda")
     d_scr = torch.empty(pkg.lde_scratch_words(nbits, ncols), dtype=torch.int64, device="cuda")
-    root_dev = pkg.commit_device(d_lde, d_tree, d_trace, nbits, nbe, ncols, 4, d_scr)
+    root_dev = pkg.commit_device(d_lde, d_tree, d_trace, nbits, nbe, ncols, arity, d_scr)
     torch.cuda.synchronize()
+    assert (root_dev == want_root).all(), ([hex(int(v)) for v in root_dev], [hex(v) for v in fx["root"]])
+    tree = d_tree.cpu().numpy().view(np.uint64)
+    assert tree.size == fx["tree_words"]
+    assert _sha(tree) == fx["tree_sha256"]
+    rows = torch.tensor(fx["sample_rows"], dtype=torch.int64, device="cuda")
+    d_rows_out = torch.empty(len(fx["sample_rows"]) * ncols, dtype=torch.int64, device="cuda")
+    pkg.lde_rows_device(d_rows_out, d_lde, NExt, ncols, rows, len(fx["sample_rows"]))
+    block = d_rows_out.cpu().numpy().view(np.uint64).reshape(-1, ncols)
+    assert [int(v) for v in block[0]] == fx["sample_row0"]
+    assert _sha(block) == fx["sample_rows_sha256"]
     host = torch.empty(N * ncols, dtype=torch.int64, pin_memory=True)
     host.copy_(d_trace)
-    del d_trace, d_lde, d_tree, d_scr
+    del d_trace, d_lde, d_tree, d_scr, d_rows_out
     torch.cuda.empty_cache()
     lib = pkg.load()
     pkg.set_hash_family(2)
-    bufs = pkg.DeviceBuffers(arity=4, n_streams=2)
+    bufs = pkg.DeviceBuffers(arity=arity, n_streams=2)
     try:
-        shape = pkg.StarkShape(nbits, nbe, ncols, 4)
+        shape = pkg.StarkShape(nbits, nbe, ncols, arity)
         params = pkg.StepsParams()
         params.trace = host.data_ptr()
         root = np.zeros(4, dtype=np.uint64)
@@ -107,4 +136,4 @@ def test_full_size_commit_witness_equals_one_pass(dev, nbits, nbe, ncols):
         assert bufs.error() == 0, lib.b200_last_error()
     finally:
         bufs.close()
-    assert (root == root_dev).all(), (root, root_dev)
+    assert (root == want_root).all(), (root, want_root)

@@ -1,11 +1,13 @@
 """Q-stage commit, LDE plan autotuner and packed-witness commit, through the C-ABI library.
 
-* Q stage: Starks::computeQ (starks.hpp:186-239) restated by the oracle; cmQ words, tree and
+* Q stage: Starks::computeQ (starks.hpp:186-239) run by the reference's own NTT and field code
+  (seeded fixtures from the reference CPU build) and restated by the oracle; cmQ words, tree and
   root bit-exact, with q given column-major or row-major.
 * Autotuner: every plan computes the same LDE (only speed changes); the table round-trips
   through a file.
 * Packed witness: a commit of the bit-packed rows equals the commit of the unpacked trace.
 """
+import hashlib
 import os
 import tempfile
 
@@ -56,6 +58,27 @@ def test_commit_q_matches_oracle(dev, torch_cuda, orc, nbits, nbe, qdeg, qdim, a
     assert (root == root_o).all()
     assert (from_dev(d_cmq).reshape(ncols, next_).T == cmq_o).all()
     assert (from_dev(d_tree) == tree_o).all()
+
+
+@pytest.mark.parametrize("rowmajor", [True, False])
+def test_commit_q_matches_reference_fixtures(dev, torch_cuda, kats, rowmajor):
+    """b200_commit_q_device against Starks::computeQ as the reference CPU build computes it
+    (tests/golden/reference_kats.json "seeded_q_commits", written by make_golden.py)."""
+    torch = torch_cuda
+    for c in kats["seeded_q_commits"]:
+        nbits, nbe, qdeg, qdim, arity = c["nBits"], c["nBitsExt"], c["qDeg"], c["qDim"], c["arity"]
+        next_ = 1 << nbe
+        q = oracle.random_field((next_, qdim), c["seed"])
+        ncols = qdeg * qdim
+        d_q = to_dev(torch, q if rowmajor else q.T.copy())
+        d_cmq = torch.zeros(next_ * ncols, dtype=torch.int64, device="cuda")
+        d_tree = torch.zeros(dev.tree_num_elements(next_, arity), dtype=torch.int64, device="cuda")
+        d_scr = torch.zeros(dev.q_scratch_words(nbe, qdim), dtype=torch.int64, device="cuda")
+        root = dev.commit_q_device(d_cmq, d_tree, d_q, nbits, nbe, qdeg, qdim, arity, d_scr, q_rowmajor=rowmajor)
+        assert [int(v) for v in root] == c["root"], c
+        cmq = np.ascontiguousarray(from_dev(d_cmq).reshape(ncols, next_).T)
+        assert hashlib.sha256(cmq.astype("<u8").tobytes()).hexdigest() == c["cmq_sha256"]
+        assert hashlib.sha256(from_dev(d_tree).astype("<u8").tobytes()).hexdigest() == c["tree_sha256"]
 
 
 def test_commit_q_rejects_bad_shapes(dev, torch_cuda):

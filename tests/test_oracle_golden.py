@@ -232,3 +232,44 @@ def test_commit_q_coefficient_chunks(orc):
         for i in range(1 << nb):
             for k in range(qdim):
                 assert int(co[i, p * qdim + k]) == int(qc[p * (1 << nb) + i, k]) * S % P
+
+
+def test_commit_q_oracle_matches_reference_fixtures(orc, kats):
+    """The oracle's computeQ restatement against the reference's own NTT/field code run on the
+    same seeded q (ref_commit_q, written into the fixtures by make_golden.py)."""
+    assert len(kats["seeded_q_commits"]) >= 5
+    for c in kats["seeded_q_commits"]:
+        q = oracle.random_field((1 << c["nBitsExt"], c["qDim"]), c["seed"])
+        root, cmq, tree = orc.commit_q(q, c["nBits"], c["nBitsExt"], c["qDeg"], c["qDim"], c["arity"])
+        assert [int(v) for v in root] == c["root"]
+        assert digest(oracle.Oracle.canon(cmq)) == c["cmq_sha256"]
+        assert digest(tree) == c["tree_sha256"]
+
+
+def test_commit_q_reference_build_reproduces_fixture(refcpu, kats):
+    c = kats["seeded_q_commits"][0]
+    q = oracle.random_field((1 << c["nBitsExt"], c["qDim"]), c["seed"])
+    root, cmq, _ = refcpu.commit_q(q, c["nBits"], c["nBitsExt"], c["qDeg"], c["qDim"], c["arity"])
+    assert [int(v) for v in root] == c["root"] and [int(v) for v in cmq[1]] == c["cmq_row1"]
+
+
+def test_seeded_generator_matches_product_host_generator(pkg, refcpu):
+    """The full-size fixtures are built from ref_fill_random; the GPU tests and bench.py fill the same
+    trace with the product's generator.  Both must give the same words (this call is host-only)."""
+    for n, seed in ((1, 0), (1000, 1000), (1 << 16, 7), (4099, 2 ** 63 + 5)):
+        assert (refcpu.fill_random(n, seed) == pkg.fill_random_host(n, seed)).all()
+
+
+def test_full_size_fixture_file():
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "full_size.json")
+    with open(path) as f:
+        shapes = {s["name"]: s for s in json.load(f)["shapes"]}
+    assert set(shapes) >= {"c2", "c4"}
+    assert (shapes["c2"]["nBits"], shapes["c2"]["nBitsExt"], shapes["c2"]["nCols"]) == (22, 23, 256)
+    assert (shapes["c4"]["nBits"], shapes["c4"]["nBitsExt"], shapes["c4"]["nCols"]) == (20, 22, 780)
+    for s in shapes.values():
+        assert len(s["root"]) == 4 and all(0 <= v < P for v in s["root"])
+        assert s["tree_words"] == oracle.tree_num_elements(1 << s["nBitsExt"], s["arity"])
+        assert len(s["sample_row0"]) == s["nCols"] and s["sample_rows"][0] == 0
