@@ -397,12 +397,12 @@ def run_ours(args, wl):
     params.trace = host.data_ptr()
     root_bufs = [np.zeros(4, dtype=np.uint64) for _ in range(args.warmup + args.steps)]
     for i in range(args.warmup):
-        lib.commit_witness(shape.ptr, ctypes.addressof(params), i, 0, 0, root_bufs[i].ctypes.data, bufs.ptr, b"")
+        lib.commit_witness(shape.setup_ptr, ctypes.addressof(params), i, 0, 0, root_bufs[i].ctypes.data, bufs.ptr, b"")
     lib.get_stream_proofs(bufs.ptr)
     barrier()
     t0 = time.perf_counter()
     for i in range(args.warmup, args.warmup + args.steps):
-        sid = lib.commit_witness(shape.ptr, ctypes.addressof(params), i, 0, 0, root_bufs[i].ctypes.data, bufs.ptr,
+        sid = lib.commit_witness(shape.setup_ptr, ctypes.addressof(params), i, 0, 0, root_bufs[i].ctypes.data, bufs.ptr,
                                  b"")
         if sid >= 2:
             raise RuntimeError(lib.b200_last_error().decode())

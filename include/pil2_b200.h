@@ -6,9 +6,9 @@
  *
  *  1. The reference's own C ABI for the commit path, same names and signatures as
  *     pil2-stark/src/api/starks_api.hpp, so the Rust crates (provers/starks-lib-c,
- *     ffi_starks.rs) can bind this library in place of libstarksgpu.a.  Where the reference
- *     passes a C++ StarkInfo/SetupCtx, this library takes the B200StarkShape below
- *     (built with b200_stark_shape_new): the four numbers the commit reads.
+ *     ffi_starks.rs) can bind this library in place of libstarksgpu.a.  stark_info_new parses
+ *     the setup's starkinfo JSON into this library's StarkInfo, and commit_witness takes
+ *     proofman's SetupC {p_stark_info, p_expressions_bin} exactly as the reference does.
  *
  *  2. A native API on device or host buffers (prefix b200_), used by the tests and the
  *     benchmark, and by callers that manage device memory themselves.
@@ -48,15 +48,13 @@ extern "C" {
  * 1. Reference C ABI (pil2-stark/src/api/starks_api.hpp)
  * ------------------------------------------------------------------------------------ */
 
-/* Shape descriptor standing in for StarkInfo / SetupCtx: nBits, nBitsExt, the committed
- * column count (mapSectionsN["cm1"] for commit_witness, nConstants for
- * calculate_const_tree) and merkleTreeArity (stark_info.cpp:24-60). */
-typedef struct B200StarkShape {
-    uint64_t nBits;
-    uint64_t nBitsExt;
-    uint64_t nCols;
-    uint64_t arity;
-} B200StarkShape;
+/* proofman's SetupC (common/src/setup.rs:45-57), which the reference reads as
+ * SetupCtx {StarkInfo &, ExpressionsBin &} (starkpil/setup_ctx.hpp:200-207).  p_stark_info comes from
+ * stark_info_new (or b200_stark_shape_new); p_expressions_bin is not read on the commit path. */
+typedef struct B200SetupC {
+    void *p_stark_info;
+    void *p_expressions_bin;
+} B200SetupC;
 
 /* Layout of StepsParams (starkpil/steps.hpp:6-20 == common/src/air_instance.rs:20-33);
  * commit_witness reads `trace` (host, row-major N x nCols). */
@@ -79,6 +77,22 @@ typedef struct B200StepsParams {
  * the reference-ABI commit entries hash with the family set here.  Must be called before them,
  * once per process (a different second value is refused, as in the reference). */
 void set_hash_family(uint8_t fam);
+
+/* starks_api.hpp:37,48 — parse a starkinfo JSON file (StarkInfo::load, stark_info.cpp:24-263) for the
+ * fields the commit path and the prover-buffer map need: starkStruct (nBits, nBitsExt, nQueries,
+ * merkleTreeArity, lastLevelVerification, verificationHashType, steps), nConstants, nPublics, nStages,
+ * qDeg, qDim, customCommits, the value/challenge/evaluation/opening maps' sizes and mapSectionsN; then
+ * lay out the prover buffer as StarkInfo::setMapOffsets does for the given flags.  Returns NULL (and
+ * b200_last_error) on a missing file or malformed JSON instead of exiting. */
+void *stark_info_new(char *filename, bool recursive_final, bool recursive, bool verify_constraints, bool verify,
+                     bool gpu, bool preallocate, bool single_use);
+void stark_info_free(void *pStarkInfo);
+/* starks_api.hpp:44-46: mapTotalN, mapTotalNCustomCommitsFixed, mapTotalNContributions of the map */
+uint64_t get_map_total_n(void *pStarkInfo);
+uint64_t get_map_total_n_custom_commits_fixed(void *pStarkInfo);
+uint64_t get_map_total_n_contributions(void *pStarkInfo);
+/* starks_api.hpp:59 — N * nConstants */
+uint64_t get_const_size(void *pStarkInfo);
 
 /* starks_api.hpp:52 — per-device set-up (twiddle/coset tables, kernel attributes) for the
  * current device.  The Poseidon2 constants are compiled in. */
@@ -105,10 +119,13 @@ uint64_t gen_device_streams(void *d_buffers, uint64_t n_streams, uint64_t n_recu
 void write_custom_commit(void *root, uint64_t arity, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols,
                          void *d_buffers, void *buffer, char *bufferFile);
 
-/* starks_api.hpp:98 — asynchronous stage-1 commit of params->trace (host, row-major).
- * pSetupCtx is a B200StarkShape*.  Returns the stream slot id (or UINT64_MAX on error); the
- * root is written to `root` when get_stream_proofs / get_stream_proofs_non_blocking harvests
- * the slot.  The host trace may be reused after wait_trace_h2d_done(d_buffers, slot). */
+/* starks_api.hpp:98 — asynchronous stage-1 commit of params->trace (host, row-major N x
+ * mapSectionsN["cm1"]).  pSetupCtx points to a B200SetupC.  The commit lands in the stream's prover
+ * buffer at the StarkInfo's mapOffsets, as commit_witness_gpu does (starks_api.cu:1599-1795): the
+ * column-major trace at ("cm1", false), the LDE at ("cm1", true), the tree at ("mt1", true)
+ * (b200_commit_buffers_aux).  Returns the stream slot id (or UINT64_MAX on error); the root is
+ * written to `root` when get_stream_proofs / get_stream_proofs_non_blocking harvests the slot.  The
+ * host trace may be reused after wait_trace_h2d_done(d_buffers, slot). */
 uint64_t commit_witness(void *pSetupCtx, void *params, uint64_t instanceId, uint64_t airgroupId, uint64_t airId,
                         void *root, void *d_buffers, char *customCommitsFixedPath);
 
@@ -127,7 +144,7 @@ void wait_trace_h2d_done(void *d_buffers, uint64_t stream_id);
 uint32_t register_host_memory(void *ptr, uint64_t size);
 void unregister_host_memory(void *ptr);
 
-/* starks_api.hpp:61 — pStarkInfo is a B200StarkShape* (nCols = nConstants).  Host const pols
+/* starks_api.hpp:61 — pStarkInfo from stark_info_new (or b200_stark_shape_new).  Host const pols
  * N x nConstants row-major in, host tree out: [LDE column-major NExt*nConstants][nodes]
  * (calculate_const_tree_gpu, starks_api.cu:1932-1980).  unified_buffer_gpu, if non-NULL, is a
  * device buffer of at least that many words used instead of a temporary allocation. */
@@ -143,8 +160,18 @@ bool set_gpu_mode(bool use_gpu);
  * 2. Native API
  * ------------------------------------------------------------------------------------ */
 
+/* A StarkInfo built from the commit's four numbers instead of a starkinfo file (nCols is both
+ * mapSectionsN["cm1"] and nConstants), with the stage-1 contribution buffer laid out as
+ * [cm1 extended][tree][cm1].  Use it as p_stark_info or pStarkInfo; free with b200_stark_shape_free. */
 void *b200_stark_shape_new(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t arity);
 void b200_stark_shape_free(void *shape);
+/* mapOffsets[(section, extended != 0)] of a StarkInfo, UINT64_MAX if absent */
+uint64_t b200_stark_info_offset(void *pStarkInfo, const char *section, int extended);
+/* a parsed field by name: nBits, nBitsExt, merkleTreeArity, lastLevelVerification, nConstants, nQueries,
+ * qDeg, qDim, or mapSectionsN.<section>; UINT64_MAX if unknown */
+uint64_t b200_stark_info_value(void *pStarkInfo, const char *name);
+/* the prover buffer of stream slot stream_id (device pointer) and the words its last commit used */
+int b200_commit_buffers_aux(void *d_buffers, uint64_t stream_id, uint64_t **d_aux, uint64_t *words);
 
 const char *b200_last_error(void);
 /* last error recorded on a d_buffers object by a void reference-ABI call (0 if none) */

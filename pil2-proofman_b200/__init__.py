@@ -45,9 +45,18 @@ _SIGS = {
     "calculate_const_tree": (None, [_vp, _vp, _vp, _vp]),
     "get_const_tree_size": (_u64, [_vp]),
     "set_gpu_mode": (ctypes.c_bool, [ctypes.c_bool]),
+    "stark_info_new": (_vp, [ctypes.c_char_p] + [ctypes.c_bool] * 7),
+    "stark_info_free": (None, [_vp]),
+    "get_map_total_n": (_u64, [_vp]),
+    "get_map_total_n_custom_commits_fixed": (_u64, [_vp]),
+    "get_map_total_n_contributions": (_u64, [_vp]),
+    "get_const_size": (_u64, [_vp]),
     # native
     "b200_stark_shape_new": (_vp, [_u64, _u64, _u64, _u64]),
     "b200_stark_shape_free": (None, [_vp]),
+    "b200_stark_info_offset": (_u64, [_vp, ctypes.c_char_p, _i32]),
+    "b200_stark_info_value": (_u64, [_vp, ctypes.c_char_p]),
+    "b200_commit_buffers_aux": (_i32, [_vp, _u64, ctypes.POINTER(_vp), _pu64]),
     "b200_last_error": (ctypes.c_char_p, []),
     "b200_buffers_error": (_i32, [_vp]),
     "b200_init": (_i32, [_i32]),
@@ -267,17 +276,62 @@ class BatchInstance(ctypes.Structure):
                 ("nCols", ctypes.c_uint64), ("arity", ctypes.c_uint64)]
 
 
-class StarkShape:
-    """Owns a B200StarkShape (stands in for StarkInfo / SetupCtx on the commit path)."""
+class SetupC(ctypes.Structure):
+    """proofman's SetupC (common/src/setup.rs:45-57): what commit_witness receives as pSetupCtx."""
+    _fields_ = [("p_stark_info", ctypes.c_void_p), ("p_expressions_bin", ctypes.c_void_p)]
 
-    def __init__(self, nbits, nbits_ext, ncols, arity):
-        self.ptr = load().b200_stark_shape_new(nbits, nbits_ext, ncols, arity)
-        self.nbits, self.nbits_ext, self.ncols, self.arity = nbits, nbits_ext, ncols, arity
+
+class StarkInfo:
+    """Owns a StarkInfo of the library: from a starkinfo JSON file (stark_info_new, starks_api.hpp:37)
+    or, with from_shape, from the commit's four numbers.  ``ptr`` is the pStarkInfo of
+    calculate_const_tree / get_const_tree_size; ``setup_ptr`` points to a SetupC holding it, the
+    pSetupCtx of commit_witness."""
+
+    def __init__(self, path=None, recursive_final=False, recursive=False, verify_constraints=False, verify=False,
+                 gpu=True, preallocate=False, single_use=False, _ptr=None):
+        lib = load()
+        if _ptr is None:
+            _ptr = lib.stark_info_new(os.fsencode(path), recursive_final, recursive, verify_constraints, verify, gpu,
+                                      preallocate, single_use)
+            if not _ptr:
+                raise B200Error(B200_EINVAL, (lib.b200_last_error() or b"").decode())
+        self.ptr = _ptr
+        self.setup = SetupC(self.ptr, None)
+        self.setup_ptr = ctypes.addressof(self.setup)
+
+    @classmethod
+    def from_shape(cls, nbits, nbits_ext, ncols, arity):
+        return cls(_ptr=load().b200_stark_shape_new(nbits, nbits_ext, ncols, arity))
+
+    def offset(self, section, extended):
+        v = int(load().b200_stark_info_offset(self.ptr, section.encode(), 1 if extended else 0))
+        return None if v == 2**64 - 1 else v
+
+    def value(self, name):
+        v = int(load().b200_stark_info_value(self.ptr, name.encode()))
+        return None if v == 2**64 - 1 else v
+
+    def map_total_n(self):
+        return int(load().get_map_total_n(self.ptr))
+
+    def map_total_n_contributions(self):
+        return int(load().get_map_total_n_contributions(self.ptr))
+
+    def close(self):
+        if getattr(self, "ptr", None) and _lib is not None:
+            _lib.stark_info_free(self.ptr)
+        self.ptr = None
 
     def __del__(self):
-        if getattr(self, "ptr", None) and _lib is not None:
-            _lib.b200_stark_shape_free(self.ptr)
-            self.ptr = None
+        self.close()
+
+
+class StarkShape(StarkInfo):
+    """A StarkInfo from the commit's four numbers (b200_stark_shape_new)."""
+
+    def __init__(self, nbits, nbits_ext, ncols, arity):
+        super().__init__(_ptr=load().b200_stark_shape_new(nbits, nbits_ext, ncols, arity))
+        self.nbits, self.nbits_ext, self.ncols, self.arity = nbits, nbits_ext, ncols, arity
 
 
 class DeviceBuffers:
@@ -293,6 +347,12 @@ class DeviceBuffers:
 
     def error(self):
         return int(load().b200_buffers_error(self.ptr))
+
+    def aux(self, stream_id):
+        """(device pointer, words) of stream slot stream_id's prover buffer (after its harvest)."""
+        p, n = ctypes.c_void_p(), ctypes.c_uint64()
+        _check(load().b200_commit_buffers_aux(self.ptr, stream_id, ctypes.byref(p), ctypes.byref(n)))
+        return p.value, n.value
 
     def close(self):
         if self.ptr:

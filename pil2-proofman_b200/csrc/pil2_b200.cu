@@ -15,6 +15,7 @@
 #include "../../include/pil2_b200.h"
 #include "merkle.cuh"
 #include "ntt.cuh"
+#include "stark_info.cuh"
 #include "stream.cuh"
 #include "synth.cuh"
 
@@ -353,27 +354,134 @@ extern "C" bool set_gpu_mode(bool use_gpu)
     return true;
 }
 
-extern "C" void *b200_stark_shape_new(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t arity)
+// ------------------------------------------------------------- StarkInfo ----
+// stark_info_new (starks_api.hpp:37): the setup's starkinfo JSON, parsed for what the commit path
+// and the prover-buffer map need (stark_info.cuh).  The flags keep the reference's meaning; they
+// shape the buffer map (gpu, preallocate, recursive, single_use, verify, verify_constraints).
+extern "C" void *stark_info_new(char *filename, bool recursive_final, bool recursive, bool verify_constraints,
+                                bool verify, bool gpu, bool preallocate, bool single_use)
 {
-    auto *s = new B200StarkShape{nBits, nBitsExt, nCols, arity};
-    return s;
+    (void)recursive_final;
+    std::string err;
+    sinfo::StarkInfo *si = sinfo::from_file(filename, err);
+    if (!si) {
+        set_err(B200_EINVAL, "stark_info_new: " + err);
+        return nullptr;
+    }
+    si->recursive = recursive;
+    si->verify_constraints = verify_constraints;
+    si->verify = verify;
+    si->gpu = gpu;
+    si->preallocate = preallocate;
+    si->singleUse = single_use;
+    sinfo::buffer_map(*si);
+    return si;
 }
 
-extern "C" void b200_stark_shape_free(void *shape) { delete (B200StarkShape *)shape; }
+extern "C" void stark_info_free(void *pStarkInfo)
+{
+    if (sinfo::StarkInfo *si = sinfo::checked(pStarkInfo)) {
+        si->magic = 0;
+        delete si;
+    }
+}
 
-// One stream slot: its own device buffers, kept resident after the commit.
+extern "C" uint64_t get_map_total_n(void *pStarkInfo)
+{
+    const sinfo::StarkInfo *si = sinfo::checked(pStarkInfo);
+    return si ? si->mapTotalN : 0;
+}
+
+extern "C" uint64_t get_map_total_n_contributions(void *pStarkInfo)
+{
+    const sinfo::StarkInfo *si = sinfo::checked(pStarkInfo);
+    return si ? si->mapTotalNContributions : 0;
+}
+
+extern "C" uint64_t get_map_total_n_custom_commits_fixed(void *pStarkInfo)
+{
+    const sinfo::StarkInfo *si = sinfo::checked(pStarkInfo);
+    return si ? si->mapTotalNCustomCommitsFixed : 0;
+}
+
+extern "C" uint64_t get_const_size(void *pStarkInfo)
+{
+    const sinfo::StarkInfo *si = sinfo::checked(pStarkInfo);
+    return si ? (1ull << si->nBits) * si->nConstants : 0;
+}
+
+extern "C" uint64_t b200_stark_info_offset(void *pStarkInfo, const char *section, int extended)
+{
+    const sinfo::StarkInfo *si = sinfo::checked(pStarkInfo);
+    if (!si || !section) return UINT64_MAX;
+    return si->offset(section, extended != 0);
+}
+
+extern "C" uint64_t b200_stark_info_value(void *pStarkInfo, const char *name)
+{
+    const sinfo::StarkInfo *si = sinfo::checked(pStarkInfo);
+    if (!si || !name) return UINT64_MAX;
+    const std::string n(name);
+    if (n == "nBits") return si->nBits;
+    if (n == "nBitsExt") return si->nBitsExt;
+    if (n == "merkleTreeArity") return si->merkleTreeArity;
+    if (n == "lastLevelVerification") return si->lastLevelVerification;
+    if (n == "nConstants") return si->nConstants;
+    if (n == "nQueries") return si->nQueries;
+    if (n == "qDeg") return si->qDeg;
+    if (n == "qDim") return si->qDim;
+    if (n.rfind("mapSectionsN.", 0) == 0) return si->sectionN(n.substr(13));
+    return UINT64_MAX;
+}
+
+extern "C" void *b200_stark_shape_new(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t arity)
+{
+    return sinfo::from_shape(nBits, nBitsExt, nCols, arity);
+}
+
+extern "C" void b200_stark_shape_free(void *shape) { stark_info_free(shape); }
+
+// One stream slot: its own device buffers, kept resident after the commit.  `d_aux` is the
+// stream's prover buffer laid out by the StarkInfo's map (the reference's d_aux_trace): after a
+// commit it holds the column-major trace at ("cm1", false), the LDE at ("cm1", true) and the tree
+// at ("mt1", true).  `d_scratch` is the LDE's work area (one column-major copy of the trace).
 struct Slot {
     cudaStream_t stream = nullptr;
     cudaStream_t copy = nullptr;  // host-to-device copies of the trace, block by block
     cudaEvent_t h2d_done = nullptr, end = nullptr;
     std::vector<cudaEvent_t> blocks;  // one per column block: that block's copy has landed
-    uint64_t *d_trace = nullptr, *d_scratch = nullptr, *d_lde = nullptr, *d_tree = nullptr;
-    uint64_t cap_trace = 0, cap_scratch = 0, cap_lde = 0, cap_tree = 0;
-    uint64_t *h_root = nullptr;  // pinned 4 words
+    uint64_t *d_aux = nullptr, *d_scratch = nullptr;
+    uint64_t cap_aux = 0, cap_scratch = 0;
+    uint64_t *d_cm1 = nullptr, *d_lde = nullptr, *d_tree = nullptr;  // views into d_aux (last commit)
+    uint64_t aux_words = 0;                                           // extent of d_aux the last commit used
+    uint64_t *h_root = nullptr;                                       // pinned 4 words
     uint64_t *user_root = nullptr;
     bool busy = false;
     uint64_t seq = 0;
 };
+
+// Word offsets of a commit's regions in the slot's prover buffer.
+struct CommitLayout {
+    uint64_t cm1_ext, mt1, cm1, words;
+};
+
+static CommitLayout commit_layout(uint64_t cm1_ext, uint64_t mt1, uint64_t cm1, uint64_t nBits, uint64_t nBitsExt,
+                                  uint64_t nCols, uint64_t arity)
+{
+    const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
+    const uint64_t tsz = merkle::tree_num_elements(NExt, arity);
+    CommitLayout l{cm1_ext, mt1, cm1, 0};
+    l.words = std::max(cm1_ext + NExt * nCols, std::max(mt1 + tsz, cm1 + N * nCols));
+    return l;
+}
+
+// the contribution buffer of a commit without a StarkInfo: [cm1 extended][tree][cm1]
+static CommitLayout packed_layout(uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t arity)
+{
+    const uint64_t NExt = 1ull << nBitsExt;
+    return commit_layout(0, NExt * nCols, NExt * nCols + merkle::tree_num_elements(NExt, arity), nBits, nBitsExt,
+                         nCols, arity);
+}
 
 struct CommitBuffers {
     int device = 0;
@@ -431,7 +539,7 @@ static void slot_destroy(Slot &s)
     if (s.stream) cudaStreamSynchronize(s.stream);
     if (s.copy) cudaStreamSynchronize(s.copy);
     for (cudaEvent_t e : s.blocks) cudaEventDestroy(e);
-    for (uint64_t *p : {s.d_trace, s.d_scratch, s.d_lde, s.d_tree})
+    for (uint64_t *p : {s.d_aux, s.d_scratch})
         if (p) cudaFree(p);
     if (s.h_root) cudaFreeHost(s.h_root);
     if (s.h2d_done) cudaEventDestroy(s.h2d_done);
@@ -535,21 +643,34 @@ static void commit_blocks(uint64_t nBits, uint64_t nCols, std::vector<uint64_t> 
     if (nCols) starts.push_back(nCols);
 }
 
-// Enqueue H2D + LDE + tree + root D2H for a row-major host trace on a slot.  The trace crosses
-// PCIe in column blocks on the slot's copy stream (a 2-D copy each, into a row-major N x B block
-// of d_trace); the compute stream transposes and extends each block as soon as it has landed, so
-// the LDE of a block overlaps the copy of the next, then hashes the rows once every column is
-// extended.  The compute stream also waits for the previously issued commit to end (see
+// Enqueue H2D + LDE + tree + root D2H for a row-major host trace on a slot, into the regions of the
+// slot's prover buffer that `lay` names.  The trace crosses PCIe in column blocks on the slot's copy
+// stream, each a 2-D copy into a row-major N x B staging block; the compute stream transposes each
+// block into ("cm1", false) as soon as it has landed and extends it into ("cm1", true), so the LDE of
+// a block overlaps the copy of the next, then hashes the rows once every column is extended.
+//
+// The staging area is the top N * nCols words of the ("cm1", true) region, as the reference stages
+// its trace in that region (commit_witness_gpu, starks_api.cu:1651-1659).  The LDE of the blocks up
+// to column x writes words [0, x * NExt) of the region, below every later block's staging, which
+// starts at (NExt - N) * nCols + x * N >= x * NExt for x <= nCols; so copies running ahead never
+// land on extended columns, and a block's own staging is overwritten only after its transpose.
+// The transposed trace stays in ("cm1", false) (the LDE reads it into the scratch), as the
+// reference's preserve_src LDE leaves it.
+//
+// The compute stream also waits for the previously issued commit to end (see
 // CommitBuffers::last_end); the copy stream only for this slot's previous commit.
 static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_t nBits, uint64_t nBitsExt,
-                       uint64_t nCols, uint64_t arity)
+                       uint64_t nCols, uint64_t arity, const CommitLayout &lay)
 {
     const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
     const uint64_t tsz = merkle::tree_num_elements(NExt, arity);
     int rc;
-    if ((rc = grow(s.d_trace, s.cap_trace, N * nCols)) || (rc = grow(s.d_scratch, s.cap_scratch, N * nCols)) ||
-        (rc = grow(s.d_lde, s.cap_lde, NExt * nCols)) || (rc = grow(s.d_tree, s.cap_tree, tsz)))
-        return rc;
+    if ((rc = grow(s.d_aux, s.cap_aux, lay.words)) || (rc = grow(s.d_scratch, s.cap_scratch, N * nCols))) return rc;
+    s.d_lde = s.d_aux + lay.cm1_ext;
+    s.d_tree = s.d_aux + lay.mt1;
+    s.d_cm1 = s.d_aux + lay.cm1;
+    s.aux_words = lay.words;
+    uint64_t *staging = s.d_lde + (NExt - N) * nCols;
     std::vector<uint64_t> starts;
     commit_blocks(nBits, nCols, starts);
     const uint64_t nblk = starts.size() - 1;
@@ -558,14 +679,14 @@ static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_
         CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
         s.blocks.push_back(e);
     }
-    // the copy may overwrite d_trace once this slot's previous commit has consumed it
+    // the copy may overwrite the staging area once this slot's previous commit is done with it
     CK(cudaStreamWaitEvent(s.copy, s.end, 0), "slot reuse");
     for (uint64_t k = 0; k < nblk; k++) {
         const uint64_t c0 = starts[k], cb = starts[k + 1] - c0;
         if (cb == nCols)
-            CK(cudaMemcpyAsync(s.d_trace, trace, N * nCols * 8, cudaMemcpyHostToDevice, s.copy), "trace H2D");
+            CK(cudaMemcpyAsync(staging, trace, N * nCols * 8, cudaMemcpyHostToDevice, s.copy), "trace H2D");
         else
-            CK(cudaMemcpy2DAsync(s.d_trace + c0 * N, cb * 8, trace + c0, nCols * 8, cb * 8, N, cudaMemcpyHostToDevice,
+            CK(cudaMemcpy2DAsync(staging + c0 * N, cb * 8, trace + c0, nCols * 8, cb * 8, N, cudaMemcpyHostToDevice,
                                  s.copy),
                "trace block H2D");
         CK(cudaEventRecord(s.blocks[k], s.copy), "event");
@@ -584,22 +705,16 @@ static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_
     for (uint64_t k = 0; k < nblk; k++) {
         const uint64_t c0 = starts[k], cb = starts[k + 1] - c0;
         CK(cudaStreamWaitEvent(s.stream, s.blocks[k], 0), "block landed");
-        if (cb == nCols) {
-            CK(ntt::lde(s.d_lde, s.d_trace, true, (uint32_t)nBits, (uint32_t)nBitsExt, nCols, s.d_scratch, s.stream),
-               "lde");
-        } else {
-            {
-                prof::Scope ps(prof::TRANSPOSE, s.stream);
-                dim3 grid((unsigned)((N + 31) / 32), (unsigned)((cb + 31) / 32));
-                ntt::transpose_kernel<<<grid, dim3(32, 8), 0, s.stream>>>(s.d_scratch + c0 * N, s.d_trace + c0 * N, N,
-                                                                          cb, N);
-                prof::count();
-                CK(cudaGetLastError(), "transpose");
-            }
-            CK(ntt::lde(s.d_lde + c0 * NExt, s.d_scratch + c0 * N, false, (uint32_t)nBits, (uint32_t)nBitsExt, cb,
-                        s.d_scratch + c0 * N, s.stream),
-               "lde");
+        {
+            prof::Scope ps(prof::TRANSPOSE, s.stream);
+            dim3 grid((unsigned)((N + 31) / 32), (unsigned)((cb + 31) / 32));
+            ntt::transpose_kernel<<<grid, dim3(32, 8), 0, s.stream>>>(s.d_cm1 + c0 * N, staging + c0 * N, N, cb, N);
+            prof::count();
+            CK(cudaGetLastError(), "transpose");
         }
+        CK(ntt::lde(s.d_lde + c0 * NExt, s.d_cm1 + c0 * N, false, (uint32_t)nBits, (uint32_t)nBitsExt, cb,
+                    s.d_scratch + c0 * N, s.stream),
+           "lde");
         if (chunked) {
             const uint64_t avail = k + 1 == nblk ? nCols : c0 + cb;  // columns extended so far
             prof::Scope ps(prof::LEAF_HASH, s.stream);
@@ -631,6 +746,8 @@ static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_
     return B200_OK;
 }
 
+// pSetupCtx is proofman's SetupC {p_stark_info, p_expressions_bin} (common/src/setup.rs:45-57), whose
+// p_stark_info came from stark_info_new or b200_stark_shape_new.
 extern "C" uint64_t commit_witness(void *pSetupCtx, void *params, uint64_t instanceId, uint64_t airgroupId,
                                    uint64_t airId, void *root, void *d_buffers, char *customCommitsFixedPath)
 {
@@ -639,18 +756,35 @@ extern "C" uint64_t commit_witness(void *pSetupCtx, void *params, uint64_t insta
     (void)airId;
     (void)customCommitsFixedPath;
     auto *b = (CommitBuffers *)d_buffers;
-    auto *shape = (const B200StarkShape *)pSetupCtx;
+    auto *setup = (const B200SetupC *)pSetupCtx;
     auto *sp = (const B200StepsParams *)params;
-    if (!b || !shape || !sp) {
+    if (!b || !setup || !sp) {
         set_err(B200_EINVAL, "commit_witness: null argument");
+        if (b) b->error = B200_EINVAL;
         return UINT64_MAX;
     }
+    const sinfo::StarkInfo *si = sinfo::checked(setup->p_stark_info);
+    if (!si) {
+        b->error = set_err(B200_EINVAL, "commit_witness: pSetupCtx->p_stark_info is not a StarkInfo of this library "
+                                        "(stark_info_new / b200_stark_shape_new)");
+        return UINT64_MAX;
+    }
+    if (si->verificationHashType != "GL") {
+        b->error = set_err(B200_EINVAL, "commit_witness: only the Goldilocks (GL) Merkle commit is provided");
+        return UINT64_MAX;
+    }
+    const uint64_t nCols = si->sectionN("cm1"), arity = si->merkleTreeArity;
     int rc = check_family();
-    if (!rc) rc = check_shape(shape->nBits, shape->nBitsExt, shape->nCols, shape->arity);
+    if (!rc) rc = check_shape(si->nBits, si->nBitsExt, nCols, arity);
+    if (!rc && (si->offset("cm1", true) == UINT64_MAX || si->offset("mt1", true) == UINT64_MAX ||
+                si->offset("cm1", false) == UINT64_MAX))
+        rc = set_err(B200_EINVAL, "commit_witness: the StarkInfo has no stage-1 buffer map (verifier layout?)");
     if (rc) {
         b->error = rc;
         return UINT64_MAX;
     }
+    const CommitLayout lay = commit_layout(si->offset("cm1", true), si->offset("mt1", true), si->offset("cm1", false),
+                                           si->nBits, si->nBitsExt, nCols, arity);
     std::lock_guard<std::mutex> lk(b->mu);
     cudaSetDevice(b->device);
     // a free slot, else the oldest in flight (harvested first)
@@ -667,7 +801,7 @@ extern "C" uint64_t commit_witness(void *pSetupCtx, void *params, uint64_t insta
         harvest(b->slots[pick]);
     }
     Slot &s = b->slots[pick];
-    rc = slot_commit(b, s, sp->trace, shape->nBits, shape->nBitsExt, shape->nCols, shape->arity);
+    rc = slot_commit(b, s, sp->trace, si->nBits, si->nBitsExt, nCols, arity, lay);
     if (rc) {
         b->error = rc;
         return UINT64_MAX;
@@ -676,6 +810,20 @@ extern "C" uint64_t commit_witness(void *pSetupCtx, void *params, uint64_t insta
     s.busy = true;
     s.seq = ++b->seq;
     return pick;
+}
+
+// The prover buffer of a stream slot (the reference's d_aux_trace of that stream) and the words its
+// last commit used: the trace, LDE and tree sit at the StarkInfo's mapOffsets.  Valid once the
+// slot's commit has been harvested.
+extern "C" int b200_commit_buffers_aux(void *d_buffers, uint64_t stream_id, uint64_t **d_aux, uint64_t *words)
+{
+    auto *b = (CommitBuffers *)d_buffers;
+    if (!b) return set_err(B200_EINVAL, "null buffers");
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (stream_id >= b->slots.size()) return set_err(B200_EINVAL, "stream id out of range");
+    if (d_aux) *d_aux = b->slots[stream_id].d_aux;
+    if (words) *words = b->slots[stream_id].aux_words;
+    return B200_OK;
 }
 
 extern "C" void get_stream_proofs(void *d_buffers)
@@ -760,16 +908,17 @@ extern "C" void write_custom_commit(void *root, uint64_t arity, uint64_t nBits, 
         harvest(s);
         const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
         const uint64_t tsz = merkle::tree_num_elements(NExt, arity);
-        rc = slot_commit(b, s, (const uint64_t *)buffer, nBits, nBitsExt, nCols, arity);
+        rc = slot_commit(b, s, (const uint64_t *)buffer, nBits, nBitsExt, nCols, arity,
+                         packed_layout(nBits, nBitsExt, nCols, arity));
         if (!rc && cudaStreamSynchronize(s.stream) != cudaSuccess) rc = set_err(B200_ECUDA, "commit failed");
         if (!rc) memcpy(r, s.h_root, 32);
         if (!rc && bufferFile && bufferFile[0]) {
             std::vector<uint64_t> host((N + NExt) * nCols + tsz);
-            // source column-major (the scratch holds the transposed trace only before the iNTT), so
-            // transpose the host buffer here; LDE and nodes come from the device.
-            const uint64_t *src = (const uint64_t *)buffer;
-            for (uint64_t c = 0; c < nCols; c++)
-                for (uint64_t i = 0; i < N; i++) host[c * N + i] = src[i * nCols + c] >= GL_P ? src[i * nCols + c] - GL_P : src[i * nCols + c];
+            // source column-major (the transposed trace the commit left in its ("cm1", false) region,
+            // canonicalised here), then LDE and nodes
+            cudaMemcpy(host.data(), s.d_cm1, N * nCols * 8, cudaMemcpyDeviceToHost);
+            for (uint64_t i = 0; i < N * nCols; i++)
+                if (host[i] >= GL_P) host[i] -= GL_P;
             cudaMemcpy(host.data() + N * nCols, s.d_lde, NExt * nCols * 8, cudaMemcpyDeviceToHost);
             cudaMemcpy(host.data() + (N + NExt) * nCols, s.d_tree, tsz * 8, cudaMemcpyDeviceToHost);
             std::ofstream f(bufferFile, std::ios::binary | std::ios::trunc);
@@ -783,20 +932,24 @@ extern "C" void write_custom_commit(void *root, uint64_t arity, uint64_t nBits, 
 
 extern "C" uint64_t get_const_tree_size(void *pStarkInfo)
 {
-    auto *sh = (const B200StarkShape *)pStarkInfo;
-    if (!sh || sh->arity < 2) return 0;
-    const uint64_t NExt = 1ull << sh->nBitsExt;
-    return NExt * sh->nCols + merkle::tree_num_elements(NExt, sh->arity);
+    const sinfo::StarkInfo *si = sinfo::checked(pStarkInfo);
+    if (!si || si->merkleTreeArity < 2 || si->verificationHashType != "GL") return 0;
+    const uint64_t NExt = 1ull << si->nBitsExt;
+    return NExt * si->nConstants + si->numNodesMT(NExt);
 }
 
+// pStarkInfo: from stark_info_new (nConstants columns) or b200_stark_shape_new (nCols columns).
 extern "C" void calculate_const_tree(void *pStarkInfo, void *pConstPolsAddress, void *pConstTree,
                                      void *unified_buffer_gpu)
 {
-    auto *sh = (const B200StarkShape *)pStarkInfo;
-    if (!sh || !pConstPolsAddress || !pConstTree) {
-        set_err(B200_EINVAL, "calculate_const_tree: null argument");
+    const sinfo::StarkInfo *si = sinfo::checked(pStarkInfo);
+    if (!si || !pConstPolsAddress || !pConstTree) {
+        set_err(B200_EINVAL, "calculate_const_tree: null argument or not a StarkInfo of this library");
         return;
     }
+    struct {
+        uint64_t nBits, nBitsExt, nCols, arity;
+    } const shape{si->nBits, si->nBitsExt, si->nConstants, si->merkleTreeArity}, *sh = &shape;
     if (check_family() || check_shape(sh->nBits, sh->nBitsExt, sh->nCols, sh->arity)) return;
     if (ensure_init_current()) return;
     const uint64_t N = 1ull << sh->nBits, NExt = 1ull << sh->nBitsExt, nCols = sh->nCols;

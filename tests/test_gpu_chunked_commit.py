@@ -38,7 +38,7 @@ def _submit(dev, lib, bufs, nb, nbe, nc, seed, keep):
     params = dev.StepsParams()
     params.trace = trace.ctypes.data
     root = np.zeros(4, dtype=np.uint64)
-    sid = lib.commit_witness(shape.ptr, ctypes.addressof(params), 0, 0, 0, root.ctypes.data, bufs.ptr, b"")
+    sid = lib.commit_witness(shape.setup_ptr, ctypes.addressof(params), 0, 0, 0, root.ctypes.data, bufs.ptr, b"")
     assert sid < 2, lib.b200_last_error()
     keep.append((shape, trace, params, root, nbe))
 
@@ -77,7 +77,7 @@ trace = oracle.random_field((1 << nb, nc), 4242)
 params = pkg.StepsParams()
 params.trace = trace.ctypes.data
 root = np.zeros(4, dtype=np.uint64)
-sid = lib.commit_witness(shape.ptr, ctypes.addressof(params), 0, 0, 0, root.ctypes.data, bufs.ptr, b"")
+sid = lib.commit_witness(shape.setup_ptr, ctypes.addressof(params), 0, 0, 0, root.ctypes.data, bufs.ptr, b"")
 lib.get_stream_proofs(bufs.ptr)
 ok = bool((root == oracle.Oracle(family=1).commit(trace, nbe, 4)[0]).all())
 err = bufs.error()
@@ -114,7 +114,7 @@ def test_commit_witness_from_registered_host_memory(dev, orc):
         params = dev.StepsParams()
         params.trace = base
         root = np.zeros(4, dtype=np.uint64)
-        assert lib.commit_witness(shape.ptr, ctypes.addressof(params), 0, 0, 0, root.ctypes.data, bufs.ptr, b"") < 2
+        assert lib.commit_witness(shape.setup_ptr, ctypes.addressof(params), 0, 0, 0, root.ctypes.data, bufs.ptr, b"") < 2
         lib.get_stream_proofs(bufs.ptr)
         assert bufs.error() == 0
         assert (root == orc.commit(np.array(trace), nbe, 4)[0]).all()

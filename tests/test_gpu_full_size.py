@@ -131,7 +131,7 @@ def test_full_size_matches_reference_cpu(dev, fx):
         params = pkg.StepsParams()
         params.trace = host.data_ptr()
         root = np.zeros(4, dtype=np.uint64)
-        assert lib.commit_witness(shape.ptr, ctypes.addressof(params), 0, 0, 0, root.ctypes.data, bufs.ptr, b"") < 2
+        assert lib.commit_witness(shape.setup_ptr, ctypes.addressof(params), 0, 0, 0, root.ctypes.data, bufs.ptr, b"") < 2
         lib.get_stream_proofs(bufs.ptr)
         assert bufs.error() == 0, lib.b200_last_error()
     finally:

@@ -211,7 +211,7 @@ def test_commit_witness_async_pool(dev, orc):
         params = dev.StepsParams()
         params.trace = trace.ctypes.data
         root = np.zeros(4, dtype=np.uint64)
-        sid = lib.commit_witness(shape.ptr, ctypes_ref(params), i, 0, 0, root.ctypes.data, bufs.ptr, b"")
+        sid = lib.commit_witness(shape.setup_ptr, ctypes_ref(params), i, 0, 0, root.ctypes.data, bufs.ptr, b"")
         assert sid < 2, dev.load().b200_last_error()
         keep.append((shape, trace, params))
         roots.append(root)
