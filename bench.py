@@ -450,6 +450,16 @@ def finish(args, wl, pkg, dist, rank, world, value, ms, launches, kernel_ms, roo
                                 "sample": sample, "root_equal": bool((cpu_root == roots[0]).all())}
         if not (cpu_root == roots[0]).all():
             raise RuntimeError("the reference CPU root of the benchmarked trace differs from the GPU root")
+    if rank == 0 and world == 1 and args.workload == "c2" and not args.no_legs:
+        # the metric's other two parts, measured in the same run: the batched mixed-size commit
+        # against the plain per-instance path, and served-stream latency
+        res = batched_vs_plain("c3", args.budget_gb)
+        line["batched"] = {k: v for k, v in res.items() if k != "workload"}
+        per_rate, npool = serve_rates([5.0], args.serve_seconds, args.pool, args.serve_budget_gb, args.slots,
+                                      args.serve_timeout, serial=False)
+        line["serve"] = dict(per_rate[0], workload="Poisson arrivals at 5 requests/s for %.0f s; shapes: %d drawn "
+                             "from the 64-instance C3 distribution (80%%) and 2^20 x 780 blowup 4 (20%%)"
+                             % (args.serve_seconds, npool - 1))
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -491,18 +501,25 @@ def instance_words(pkg, nb, nbe, nc, arity=4):
     return N * nc, N * nc, NExt * nc, pkg.tree_num_elements(NExt, arity)
 
 
-def run_batched(args):
-    """Batched mixed-size commit (64 instances) vs the plain one-instance-at-a-time path, same data,
-    same device, waves bounded by a device-memory budget; roots compared bit for bit."""
+def batched_vs_plain(workload, budget_gb, autotune=False):
+    """Batched mixed-size commit vs the plain one-instance-at-a-time path on the same data and device,
+    in waves bounded by a device-memory budget; roots compared bit for bit.  Returns a dict."""
     import torch
 
     pkg = load_package()
     pkg.init(0)
     lib = pkg.load()
     dev = torch.device("cuda", 0)
-    make_shapes, shapes_desc = BATCH_SETS[args.workload]
+    make_shapes, shapes_desc = BATCH_SETS[workload]
     shapes = make_shapes()
-    budget = int(args.budget_gb * 2**30) // 8  # words
+    tuned = {}
+    if autotune:  # untimed set-up: a plan per distinct (nBits, nBitsExt, column bucket)
+        for nb, nbe, nc in shapes:
+            key = (nb, nbe, 0 if nc <= 32 else 1 if nc <= 128 else 2 if nc <= 512 else 3)
+            if key not in tuned:
+                t_ms, kf, kr = pkg.autotune_lde(nb, nbe, nc)
+                tuned[key] = (kf, kr)
+    budget = int(budget_gb * 2**30) // 8  # words
     waves, cur, used = [], [], 0
     for i, (nb, nbe, nc) in enumerate(shapes):
         w = sum(instance_words(pkg, nb, nbe, nc))
@@ -556,7 +573,6 @@ def run_batched(args):
                 raise RuntimeError(lib.b200_last_error().decode())
             roots_batch = np.zeros((len(wave), 4), dtype=np.uint64)
             for rep in range(2):
-                l0 = pkg.launch_count()
                 ev0.record(stream)
                 rc = lib.b200_batch_plan_run(plan, roots_batch.ctypes.data, stream.cuda_stream, 1)
                 ev1.record(stream)
@@ -569,8 +585,9 @@ def run_batched(args):
         mismatches += int((roots_plain != roots_batch).any(axis=1).sum())
         del arena
         torch.cuda.empty_cache()
-    line = {
-        "metric": METRIC + " - batched vs plain", "workload": args.workload,
+    return {
+        "workload": workload, "desc": shapes_desc + ", Poseidon2 W16 arity 4, device budget %.0f GiB per wave"
+        % budget_gb,
         "value": round(total_elems / (t_batch * 1e-3) / 1e9, 4), "unit": UNIT,
         "plain_value": round(total_elems / (t_plain * 1e-3) / 1e9, 4),
         "batched_over_plain": round(t_plain / t_batch, 4),
@@ -578,87 +595,142 @@ def run_batched(args):
         "instances": len(shapes), "waves": len(waves), "total_lde_elements": total_elems,
         "launches_plain": launches_plain, "launches_batched": launches_batch,
         "roots_bit_exact": mismatches == 0, "mismatched_roots": mismatches,
-        "config": {"workload": shapes_desc + ", Poseidon2 W16 arity 4, device budget %.0f GiB per wave"
-                   % args.budget_gb},
-        "n_gpus": 1, "higher_is_better": True, "dtype": "u64", "data": "synthetic (seeded uniform Goldilocks)",
+        "ntt_plans": {"%d/%d/%d" % k: list(v) for k, v in tuned.items()} if tuned else "default",
     }
+
+
+def run_batched(args):
+    res = batched_vs_plain(args.workload, args.budget_gb, args.autotune)
+    line = {"metric": METRIC + " - batched vs plain", "workload": args.workload, "value": res["value"], "unit": UNIT,
+            "config": {"workload": res["desc"]}, "n_gpus": 1, "higher_is_better": True, "dtype": "u64",
+            "data": "synthetic (seeded uniform Goldilocks)"}
+    line.update({k: v for k, v in res.items() if k not in ("value", "desc", "workload")})
     print(json.dumps(line), flush=True)
-    return 0 if mismatches == 0 else 1
+    return 0 if res["roots_bit_exact"] else 1
 
 
-def run_serving(args):
-    """Served request stream (C5): Poisson arrivals at each rate, request shapes drawn from the C3
-    distribution with a fifth shaped like C4, admitted by the commit server under a device-memory
-    budget; each request's LDE and tree stay resident until it completes and is released.  Reports
-    throughput and p50/p99 request latency (submission to completion) per rate."""
+def serve_pool(lib, n_c3, seed=12):
+    """Request shapes: n_c3 drawn from the 64-instance C3 distribution and the C4 shape (2^20 x 780,
+    blowup 4), each with one seeded pinned host trace."""
     import torch
 
-    pkg = load_package()
-    pkg.init(0)
-    lib = pkg.load()
-    rng = np.random.Generator(np.random.PCG64(11))
-    pool = c3_shapes(seed=12, n=args.pool) + [(20, 22, 780)]
+    pool = c3_shapes(seed=seed, n=n_c3) + [(20, 22, 780)]
     hosts = []
     for i, (nb, nbe, nc) in enumerate(pool):
         h = torch.empty((1 << nb) * nc, dtype=torch.int64, pin_memory=True)
         lib.b200_fill_random_host(h.data_ptr(), h.numel(), 7000 + i)
         hosts.append(h)
-    lines = []
-    for rate in [float(r) for r in args.rates.split(",")]:
-        nreq = max(1, min(args.requests, int(rate * args.duration)))
-        picks = [len(pool) - 1 if rng.random() < 0.2 else int(rng.integers(0, len(pool) - 1)) for _ in range(nreq)]
-        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
-        srv = lib.b200_server_new(0, int(args.serve_budget_gb * 2**30), args.slots)
-        if not srv:
+    return pool, hosts
+
+
+def serve_stream(lib, pool, hosts, arrivals, picks, mode, budget_gb, slots, timeout_s):
+    """Submit requests at the given arrival times to a commit server (mode 1 continuous batching,
+    0 FIFO); returns (latencies ms, wall s, roots, stats)."""
+    nreq = len(picks)
+    srv = lib.b200_server_new(0, int(budget_gb * 2**30), slots)
+    if not srv:
+        raise RuntimeError(lib.b200_last_error().decode())
+    roots = np.zeros((nreq, 4), dtype=np.uint64)
+    ids, lat, done = [None] * nreq, [None] * nreq, 0
+    lat_c = ctypes.c_double()
+    try:
+        if lib.b200_server_configure(srv, mode, 1 << 26, 64) != 0:
             raise RuntimeError(lib.b200_last_error().decode())
-        roots = np.zeros((nreq, 4), dtype=np.uint64)
-        ids, lat, done = [None] * nreq, [None] * nreq, 0
         t0 = time.perf_counter()
         nxt = 0
-        lat_c = ctypes.c_double()
-        try:
-            while done < nreq:
-                now = time.perf_counter() - t0
-                while nxt < nreq and arrivals[nxt] <= now:
-                    nb, nbe, nc = pool[picks[nxt]]
-                    rid = lib.b200_server_submit(srv, hosts[picks[nxt]].data_ptr(), nb, nbe, nc, 4,
-                                                 roots[nxt].ctypes.data)
-                    if rid < 0:
-                        raise RuntimeError(lib.b200_last_error().decode())
-                    ids[nxt] = rid
-                    nxt += 1
-                for i in range(nxt):
-                    if lat[i] is None:
-                        st = lib.b200_server_status(srv, ids[i], ctypes.byref(lat_c))
-                        if st < 0:
-                            raise RuntimeError("status %d: %s" % (st, lib.b200_last_error().decode()))
-                        if st == 1:
-                            lat[i] = lat_c.value
-                            lib.b200_server_release(srv, ids[i])  # frees its device memory
-                            done += 1
-                if now > args.serve_timeout:
-                    raise RuntimeError("served stream did not finish within %.0f s" % args.serve_timeout)
-                time.sleep(0.001)
-            wall = time.perf_counter() - t0
-        finally:
-            lib.b200_server_free(srv)
-        # same shape, same trace -> same root
-        for k in range(len(pool)):
-            rk = [roots[i] for i in range(nreq) if picks[i] == k]
-            if rk and not all((r == rk[0]).all() for r in rk):
-                raise RuntimeError("served roots differ for one input")
+        while done < nreq:
+            now = time.perf_counter() - t0
+            while nxt < nreq and arrivals[nxt] <= now:
+                nb, nbe, nc = pool[picks[nxt]]
+                rid = lib.b200_server_submit(srv, hosts[picks[nxt]].data_ptr(), nb, nbe, nc, 4, roots[nxt].ctypes.data)
+                if rid < 0:
+                    raise RuntimeError(lib.b200_last_error().decode())
+                ids[nxt] = rid
+                nxt += 1
+            for i in range(nxt):
+                if lat[i] is None:
+                    st = lib.b200_server_status(srv, ids[i], ctypes.byref(lat_c))
+                    if st < 0:
+                        raise RuntimeError("status %d: %s" % (st, lib.b200_last_error().decode()))
+                    if st == 1:
+                        lat[i] = lat_c.value
+                        lib.b200_server_release(srv, ids[i])  # frees its device memory
+                        done += 1
+            if now > timeout_s:
+                raise RuntimeError("served stream did not finish within %.0f s" % timeout_s)
+            time.sleep(0.001)
+        wall = time.perf_counter() - t0
+        st = (ctypes.c_uint64 * 5)()
+        lib.b200_server_stats(srv, st, 5)
+        times = (ctypes.c_double * 3)()
+        waits, service = [], []
+        for rid in ids:
+            lib.b200_server_request_times(srv, rid, times)
+            waits.append(times[1] - times[0])
+            service.append(times[2] - times[1])
+        stats = {"plain_units": st[0], "batched_units": st[1], "batched_requests": st[2], "pool_trims": st[3],
+                 "overtakes": st[4], "mean_wait_to_admission_ms": round(float(np.mean(waits)), 2),
+                 "mean_admission_to_done_ms": round(float(np.mean(service)), 2)}
+    finally:
+        lib.b200_server_free(srv)
+    return lat, wall, roots, stats
+
+
+def serve_rates(rates, duration, n_c3, budget_gb, slots, timeout_s, serial=True):
+    """Poisson request streams at each rate for `duration` seconds of arrivals, served by the
+    continuous-batching server and by the FIFO server on the same arrivals; p50/p99 latency and
+    GElem/s of each, and the GElem/s of serial plain commits of the same request list."""
+    pkg = load_package()
+    pkg.init(0)
+    lib = pkg.load()
+    pool, hosts = serve_pool(lib, n_c3)
+    rng = np.random.Generator(np.random.PCG64(11))
+    out = []
+    for rate in rates:
+        nreq = max(1, int(round(rate * duration)))
+        picks = [len(pool) - 1 if rng.random() < 0.2 else int(rng.integers(0, len(pool) - 1)) for _ in range(nreq)]
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
         elems = sum((1 << pool[p][1]) * pool[p][2] for p in picks)
-        lines.append({"rate_per_s": rate, "requests": nreq, "wall_s": round(wall, 3),
-                      "throughput_gelem_s": round(elems / wall / 1e9, 4),
-                      "p50_ms": round(float(np.percentile(lat, 50)), 2),
-                      "p99_ms": round(float(np.percentile(lat, 99)), 2),
-                      "max_ms": round(float(np.max(lat)), 2)})
-    line = {"metric": "served commit stream: request latency p50/p99 and throughput", "workload": "c5",
-            "unit": "ms", "value": lines[0]["p99_ms"], "higher_is_better": False, "per_rate": lines,
-            "config": {"workload": "Poisson arrivals; shapes: %d drawn from the 64-instance C3 distribution "
-                                   "(80%%) and 2^20 x 780 blowup 4 (20%%); Poseidon2 W16 arity 4" % args.pool,
-                       "device_budget_gib": args.serve_budget_gb, "slots": args.slots,
-                       "requests_per_rate": "min(%d, rate x %.0f s)" % (args.requests, args.duration)},
+        entry = {"rate_per_s": rate, "requests": nreq, "arrivals_s": round(float(arrivals[-1]), 2)}
+        all_roots = []
+        for mode, name in ((1, "continuous_batching"), (0, "fifo")):
+            lat, wall, roots, stats = serve_stream(lib, pool, hosts, arrivals, picks, mode, budget_gb, slots,
+                                                   timeout_s)
+            all_roots.append(roots)
+            entry[name] = {"wall_s": round(wall, 3), "throughput_gelem_s": round(elems / wall / 1e9, 4),
+                           "p50_ms": round(float(np.percentile(lat, 50)), 2),
+                           "p99_ms": round(float(np.percentile(lat, 99)), 2),
+                           "max_ms": round(float(np.max(lat)), 2), **stats}
+        if serial:
+            # the same request list as plain commits one after another, all queued at time 0
+            _, wall, roots, _ = serve_stream(lib, pool, hosts, np.zeros(nreq), picks, 0, budget_gb, 1, timeout_s)
+            all_roots.append(roots)
+            entry["serial_plain"] = {"wall_s": round(wall, 3), "throughput_gelem_s": round(elems / wall / 1e9, 4)}
+        # every served root equals the root of the same trace served any other way
+        for k in range(len(pool)):
+            rk = [r[i] for r in all_roots for i in range(nreq) if picks[i] == k]
+            if rk and not all((x == rk[0]).all() for x in rk):
+                raise RuntimeError("served roots differ for one input")
+        entry["roots_consistent"] = True
+        out.append(entry)
+    del hosts
+    return out, len(pool)
+
+
+def run_serving(args):
+    """Served request stream (C5): Poisson arrivals at each rate, request shapes drawn from the C3
+    distribution with a fifth shaped like C4, admitted by the commit server under a device-memory
+    budget; each request's LDE and tree stay resident until it completes and is released."""
+    rates = [float(r) for r in args.rates.split(",")]
+    per_rate, npool = serve_rates(rates, args.duration, args.pool, args.serve_budget_gb, args.slots,
+                                  args.serve_timeout)
+    line = {"metric": "served commit stream: request latency p50/p99 and throughput, continuous batching vs FIFO",
+            "workload": "c5", "unit": "ms", "value": per_rate[0]["continuous_batching"]["p99_ms"],
+            "higher_is_better": False, "per_rate": per_rate,
+            "config": {"workload": "Poisson arrivals for %.0f s per rate; shapes: %d drawn from the 64-instance C3 "
+                                   "distribution (80%%) and 2^20 x 780 blowup 4 (20%%); Poseidon2 W16 arity 4"
+                                   % (args.duration, npool - 1),
+                       "device_budget_gib": args.serve_budget_gb, "slots": args.slots},
             "n_gpus": 1, "dtype": "u64", "data": "synthetic (seeded uniform Goldilocks)"}
     print(json.dumps(line), flush=True)
     return 0
@@ -817,12 +889,15 @@ def main():
     ap.add_argument("--hash-family", type=int, choices=[1, 2], default=2,
                     help="1 = Poseidon1, 2 = Poseidon2 (single-instance workloads)")
     ap.add_argument("--rates", default="5,20,80", help="c5: Poisson arrival rates per second")
-    ap.add_argument("--duration", type=float, default=10.0, help="c5: seconds of arrivals per rate")
-    ap.add_argument("--requests", type=int, default=120, help="c5: at most this many requests per rate")
-    ap.add_argument("--pool", type=int, default=6, help="c5: distinct C3-distributed request shapes")
-    ap.add_argument("--slots", type=int, default=4, help="c5: concurrent server slots")
+    ap.add_argument("--duration", type=float, default=60.0, help="c5: seconds of arrivals per rate")
+    ap.add_argument("--pool", type=int, default=12, help="c5: distinct C3-distributed request shapes")
+    ap.add_argument("--slots", type=int, default=2, help="c5: server slots (units admitted at once)")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0, help="c5: server device-memory budget")
-    ap.add_argument("--serve-timeout", type=float, default=300.0, help="c5: give up after this many seconds")
+    ap.add_argument("--serve-timeout", type=float, default=1800.0, help="c5: give up after this many seconds")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="default workload: skip the batched (c3) and served (c5) legs of the JSON line")
+    ap.add_argument("--serve-seconds", type=float, default=30.0,
+                    help="default workload: seconds of arrivals of its served leg (5 requests/s)")
     args = ap.parse_args()
     if args.workload in BATCH_SETS:
         return run_batched(args)

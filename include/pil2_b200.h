@@ -208,9 +208,14 @@ int b200_lde_device(uint64_t *d_lde, const uint64_t *d_trace, int trace_rowmajor
  * buffer).  The scratch is a 64 MiB array inside this library's image, held by every GPU
  * that loads the library until exit: N * nCols must be <= 2^23 (larger shapes return
  * B200_EINVAL).  No cudaMalloc / cudaFree or other allocating call is made (with the
- * optional kernel timers off, the default).  The first call on a device resolves the
- * array's device address and uploads the twiddle tables; make that first call before any
- * stream capture.  All calls share the one array, which keeps the last call's contents
+ * optional kernel timers off, the default).  The array is part of the library's device image:
+ * the driver reserves its 64 MiB when it loads that image on a device, which with lazy module
+ * loading (CUDA_MODULE_LOADING=LAZY) happens at the first call into the library there (this one,
+ * b200_init or any other) — call b200_init(device) at set-up to pay it then.  The first call of
+ * this entry point on a device resolves the array's device address and uploads the twiddle
+ * tables; make that first call before any stream capture.  The address is kept per device for the
+ * life of the process: cudaDeviceReset is not supported (nor is it for the library's other
+ * per-device state).  All calls share the one array, which keeps the last call's contents
  * (nothing in it needs to start at zero): calls that overlap on the GPU — on different
  * streams or from different threads — race and must be serialised by the caller. */
 int b200_lde_device_static_scratch(uint64_t *d_lde, const uint64_t *d_trace, int trace_rowmajor, uint64_t nBits,
@@ -266,14 +271,28 @@ void b200_batch_plan_free(void *plan);
 uint64_t b200_batch_plan_launches(void *plan);
 int b200_commit_batch_device(const B200BatchInstance *inst, uint64_t n, uint64_t *roots_host, void *stream);
 
-/* ---- Commit server (continuous admission) ----------------------------------------------
- * Requests (host row-major traces; pinned memory lets the copies overlap) are admitted in
- * arrival order whenever one of `slots` streams is free and the request's device buffers fit
- * in `budget_bytes`; admitted requests run concurrently on their own streams.  The LDE and
- * tree of a finished request stay on the device (b200_server_buffers, for query reads) until
- * b200_server_release.  The reference's stream pool + selectStream + get_stream_proofs loop
- * (starks_api.cu:1138-1170, 2665-...) is the single-request counterpart. */
+/* ---- Commit server (continuous batching) ------------------------------------------------
+ * Requests (host row-major traces; pinned memory lets the copies overlap) are admitted as soon
+ * as one of `slots` slots is free and the request's device buffers fit in `budget_bytes` (the
+ * server's own memory pool); an admitted unit's host-to-device copy overlaps the kernels of the
+ * units ahead of it, and the units' kernels run in admission order.  The small requests waiting
+ * together (LDE of at most small_elems elements) are admitted as one batched unit (one
+ * b200_batch_plan over all of them) and may pass waiting large requests, each of which is passed
+ * at most four times.  The LDE and tree of a finished request stay on the device
+ * (b200_server_buffers, for query reads) until b200_server_release.  The reference's stream pool
+ * + selectStream + get_stream_proofs loop (starks_api.cu:1138-1170, 2665-...) is the
+ * one-request-per-stream counterpart. */
 void *b200_server_new(int device, uint64_t budget_bytes, uint32_t slots);
+/* Before the first submit: batching 1 (default) as above, 0 = FIFO (every request a plain unit in
+ * arrival order; the comparison point); small_elems (default 2^26) and max_batch (requests per
+ * batched unit, default 64). */
+int b200_server_configure(void *srv, int batching, uint64_t small_elems, uint32_t max_batch);
+/* counters into out[0..n): plain units, batched units, requests in batched units, pool trims (an
+ * admission that did not fit the pool's cached blocks), times a waiting request was passed */
+int b200_server_stats(void *srv, uint64_t *out, uint64_t n);
+/* submission, admission and completion time of a request in ms since the server was created
+ * (times3[1], times3[2] = -1 until reached) */
+int b200_server_request_times(void *srv, int64_t id, double *times3);
 /* returns a request id > 0, or B200_EBUSY if the request can never fit the budget */
 int64_t b200_server_submit(void *srv, const uint64_t *host_trace, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols,
                            uint64_t arity, uint64_t *root_out);
@@ -298,6 +317,14 @@ const char *b200_timing_name(int category);
 
 /* Kernels launched by this library since the process started. */
 uint64_t b200_launch_count(void);
+
+/* Row-major -> column-major transposes: 1 (default) stages the tiles with the Tensor Memory
+ * Accelerator where the source is 16-byte aligned with an even column count, 0 always uses the
+ * thread-loaded shared-memory tiles.  Same values either way; returns the previous setting. */
+int b200_set_transpose_tma(int on);
+/* 1 if a TMA transpose tile copy did not land within the kernel's wait bound since the last call
+ * (the flag is then reset), 0 otherwise, < 0 on a CUDA error. */
+int b200_tma_wait_errors(void);
 
 /* INT32 multiply-add throughput probe: `blocks` x 256 threads each run 8 independent
  * mad.lo/mad.hi chains of `iters` steps; returns the measured rate in G IMAD/s. */

@@ -82,6 +82,8 @@ _SIGS = {
     "b200_timing_get": (_i32, [_i32, ctypes.POINTER(ctypes.c_double), _pu64]),
     "b200_timing_name": (ctypes.c_char_p, [_i32]),
     "b200_launch_count": (_u64, []),
+    "b200_set_transpose_tma": (_i32, [_i32]),
+    "b200_tma_wait_errors": (_i32, []),
     "b200_probe_imad": (_i32, [_u64, _u64, ctypes.POINTER(ctypes.c_double)]),
     "b200_batch_plan_new": (_vp, [_vp, _u64]),
     "b200_batch_plan_run": (_i32, [_vp, _vp, _vp, _i32]),
@@ -95,6 +97,9 @@ _SIGS = {
     "b200_server_release": (_i32, [_vp, ctypes.c_int64]),
     "b200_server_buffers": (_i32, [_vp, ctypes.c_int64, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "b200_server_free": (None, [_vp]),
+    "b200_server_configure": (_i32, [_vp, _i32, _u64, ctypes.c_uint32]),
+    "b200_server_stats": (_i32, [_vp, _pu64, _u64]),
+    "b200_server_request_times": (_i32, [_vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)]),
     # query openings, Q stage, plan autotuner, packed witness
     "b200_query_proof_words": (_u64, [_u64, _u64, _u64, _u64]),
     "b200_query_openings_device": (_i32, [_vp, _vp, _u64, _u64, _vp, _u64, _u64, _vp, _u64, _vp]),

@@ -235,14 +235,16 @@ class Plan {
     cudaGraphExec_t graph = nullptr;
     int leaf_ctas = 0;
     int family = 2;  // hash family of the leaves and levels (1 = Poseidon1, 2 = Poseidon2)
+    // d_table and h_roots belong to the caller (the commit server's pool and pinned staging)
+    bool borrowed = false;
 
     ~Plan() { release(); }
 
     void release()
     {
         if (graph) cudaGraphExecDestroy(graph);
-        if (d_table) cudaFree(d_table);
-        if (h_roots) cudaFreeHost(h_roots);
+        if (d_table && !borrowed) cudaFree(d_table);
+        if (h_roots && !borrowed) cudaFreeHost(h_roots);
         graph = nullptr;
         d_table = nullptr;
         h_roots = nullptr;
@@ -496,9 +498,8 @@ class Plan {
             case 7: {
                 const Inst &x = inst[(size_t)L.inst];
                 const uint64_t N = 1ull << x.nBits;
-                const dim3 grid((unsigned)((N + 31) / 32), (unsigned)((x.nCols + 31) / 32));
-                ntt::transpose_kernel<<<grid, dim3(32, 8), 0, s>>>(x.scratch, x.trace, N, x.nCols, N);
-                break;
+                if ((e = ntt::transpose(x.scratch, x.trace, N, x.nCols, N, s)) != cudaSuccess) return e;
+                continue;  // transpose counts its launch
             }
             case 1: pass_grouped<<<(unsigned)L.blocks, 512, L.smem, s>>>((const PassEntry *)ent, L.n); break;
             case 5: {

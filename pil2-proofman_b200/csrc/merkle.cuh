@@ -45,6 +45,23 @@ __device__ __forceinline__ void permute_fam(uint64_t *st)
         p2::permute_smem<W, TPB>(st);
 }
 
+// Digest i of a level sits at base + 4*i words, so every digest has the base's alignment.  A
+// 16-byte aligned base takes two 16-byte stores / loads per digest, any other base (a tree at an odd
+// word offset of a caller's buffer) four 8-byte ones; the test is uniform across the launch.
+__device__ __forceinline__ void store_digest(uint64_t *d, const uint64_t *st)
+{
+    const uint64_t a = gl::canon(st[0]), b = gl::canon(st[TPB]), c = gl::canon(st[2 * TPB]), e = gl::canon(st[3 * TPB]);
+    if ((reinterpret_cast<uintptr_t>(d) & 15) == 0) {
+        reinterpret_cast<ulonglong2 *>(d)[0] = make_ulonglong2(a, b);
+        reinterpret_cast<ulonglong2 *>(d)[1] = make_ulonglong2(c, e);
+    } else {
+        d[0] = a;
+        d[1] = b;
+        d[2] = c;
+        d[3] = e;
+    }
+}
+
 // Sponge of one row; st = this thread's state slot in a W x TPB shared array.
 template <int W, int FAM = 2>
 __device__ __forceinline__ void leaf_row(uint64_t *st, uint64_t *__restrict__ digests,
@@ -70,10 +87,8 @@ __device__ __forceinline__ void leaf_row(uint64_t *st, uint64_t *__restrict__ di
         }
         permute_fam<W, FAM>(st);
     }
-    uint64_t *d = digests + row * 4;
     // ncols == 0 leaves the state zeroed: the zero digest
-    reinterpret_cast<ulonglong2 *>(d)[0] = make_ulonglong2(gl::canon(st[0]), gl::canon(st[TPB]));
-    reinterpret_cast<ulonglong2 *>(d)[1] = make_ulonglong2(gl::canon(st[2 * TPB]), gl::canon(st[3 * TPB]));
+    store_digest(digests + row * 4, st);
 }
 
 template <int W, int FAM = 2>
@@ -97,12 +112,18 @@ __device__ __forceinline__ void node_one(uint64_t *st, uint64_t *__restrict__ le
     for (int c = 0; c < ARITY; c++) {
         const uint64_t child = i * ARITY + c;
         if (child < pending) {
-            const ulonglong2 *q = reinterpret_cast<const ulonglong2 *>(level + child * 4);
-            const ulonglong2 v0 = q[0], v1 = q[1];
-            st[(4 * c + 0) * TPB] = v0.x;
-            st[(4 * c + 1) * TPB] = v0.y;
-            st[(4 * c + 2) * TPB] = v1.x;
-            st[(4 * c + 3) * TPB] = v1.y;
+            const uint64_t *q = level + child * 4;
+            if ((reinterpret_cast<uintptr_t>(q) & 15) == 0) {
+                const ulonglong2 v0 = reinterpret_cast<const ulonglong2 *>(q)[0],
+                                 v1 = reinterpret_cast<const ulonglong2 *>(q)[1];
+                st[(4 * c + 0) * TPB] = v0.x;
+                st[(4 * c + 1) * TPB] = v0.y;
+                st[(4 * c + 2) * TPB] = v1.x;
+                st[(4 * c + 3) * TPB] = v1.y;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; j++) st[(4 * c + j) * TPB] = q[j];
+            }
         } else {
 #pragma unroll
             for (int j = 0; j < 4; j++) st[(4 * c + j) * TPB] = 0;
@@ -112,9 +133,7 @@ __device__ __forceinline__ void node_one(uint64_t *st, uint64_t *__restrict__ le
         for (uint64_t z = 0; z < pad * 4; z++) level[pending * 4 + z] = 0;
     }
     permute_fam<W, FAM>(st);
-    uint64_t *d = out + i * 4;
-    reinterpret_cast<ulonglong2 *>(d)[0] = make_ulonglong2(gl::canon(st[0]), gl::canon(st[TPB]));
-    reinterpret_cast<ulonglong2 *>(d)[1] = make_ulonglong2(gl::canon(st[2 * TPB]), gl::canon(st[3 * TPB]));
+    store_digest(out + i * 4, st);
 }
 
 template <int W, int FAM = 2>

@@ -22,7 +22,9 @@
 #pragma once
 #include "gl64.cuh"
 #include "prof.cuh"
+#include "transpose_tma.cuh"
 
+#include <atomic>
 #include <map>
 #include <mutex>
 
@@ -558,6 +560,30 @@ __global__ void __launch_bounds__(256) transpose_kernel(uint64_t *__restrict__ d
 
 // ------------------------------------------------------------------ host side ----
 
+// 1 (default): row-major -> column-major transposes stage their tiles with the TMA
+// (transpose_tma_kernel) where the shape and alignment allow it; 0: shared-memory tiles loaded by
+// the threads (transpose_kernel).  Same values either way.
+inline std::atomic<int> &transpose_tma_enabled()
+{
+    static std::atomic<int> on{1};
+    return on;
+}
+
+// row-major nrows x ncols -> column-major with column stride dst_cs (one launch)
+inline cudaError_t transpose(uint64_t *dst, const uint64_t *src, uint64_t nrows, uint64_t ncols, uint64_t dst_cs,
+                             cudaStream_t stream)
+{
+    if (nrows == 0 || ncols == 0) return cudaSuccess;
+    const dim3 grid((unsigned)((nrows + 31) / 32), (unsigned)((ncols + 31) / 32));
+    CUtensorMap map;
+    if (transpose_tma_enabled().load() && tma_source_map(&map, src, nrows, ncols))
+        transpose_tma_kernel<<<grid, dim3(32, 8), 0, stream>>>(dst, map, nrows, ncols, dst_cs);
+    else
+        transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(dst, src, nrows, ncols, dst_cs);
+    prof::count();
+    return cudaGetLastError();
+}
+
 struct Window {
     uint32_t s0, k, lgL;
 };
@@ -652,7 +678,11 @@ inline cudaError_t launch_pass(const Pass &p, uint64_t ncols, cudaStream_t strea
 inline uint64_t lde_scratch_words(uint32_t nBits, uint64_t ncols) { return (1ull << nBits) * ncols; }
 
 // d_lde: column-major NExt x ncols (stride NExt).  d_trace: row-major (trace_rowmajor) or
-// column-major with stride N.  d_scratch: lde_scratch_words() words, distinct from both.
+// column-major with stride N.  d_scratch: lde_scratch_words() words, distinct from d_lde.  For
+// column-major input d_scratch may be d_trace itself: every inverse window reads a whole tile
+// before writing it back, so the transform then runs in place and leaves the coefficients there;
+// with d_scratch distinct the input is left unchanged.  Row-major input is transposed into
+// d_scratch first, so there d_scratch must not overlap d_trace.
 inline cudaError_t lde(uint64_t *d_lde, const uint64_t *d_trace, bool trace_rowmajor, uint32_t nBits,
                        uint32_t nBitsExt, uint64_t ncols, uint64_t *d_scratch, cudaStream_t stream)
 {
@@ -666,10 +696,7 @@ inline cudaError_t lde(uint64_t *d_lde, const uint64_t *d_trace, bool trace_rowm
     uint64_t cur_cs = N;
     if (trace_rowmajor) {
         prof::Scope ps(prof::TRANSPOSE, stream);
-        dim3 grid((unsigned)((N + 31) / 32), (unsigned)((ncols + 31) / 32));
-        transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(d_scratch, d_trace, N, ncols, N);
-        prof::count();
-        if ((err = cudaGetLastError()) != cudaSuccess) return err;
+        if ((err = transpose(d_scratch, d_trace, N, ncols, N, stream)) != cudaSuccess) return err;
         cur = d_scratch;
     }
 
@@ -741,9 +768,7 @@ inline cudaError_t lde_q(uint64_t *d_cmq, const uint64_t *d_q, bool q_rowmajor, 
     cudaError_t err;
     if (q_rowmajor) {
         prof::Scope ps(prof::TRANSPOSE, stream);
-        dim3 grid((unsigned)((NExt + 31) / 32), (unsigned)((qDim + 31) / 32));
-        transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(d_scratch, d_q, NExt, qDim, NExt);
-        prof::count();
+        if ((err = transpose(d_scratch, d_q, NExt, qDim, NExt, stream)) != cudaSuccess) return err;
     } else {
         err = cudaMemcpyAsync(d_scratch, d_q, NExt * qDim * 8, cudaMemcpyDeviceToDevice, stream);
         if (err != cudaSuccess) return err;

@@ -278,7 +278,7 @@ extern "C" void b200_fill_random_host(uint64_t *buf, uint64_t n, uint64_t seed)
 
 extern "C" const char *b200_kernel_names(void)
 {
-    return "pass16_kernel\ntranspose_kernel\nleaf_hash_kernel\nnode_kernel\npermute_kernel\nlde_rows_kernel\n"
+    return "pass16_kernel\ntranspose_kernel\ntranspose_tma_kernel\nleaf_hash_kernel\nnode_kernel\npermute_kernel\nlde_rows_kernel\n"
            "fill_kernel\nimad_probe_kernel\ntranspose_grouped\npass_grouped\nleaf_persistent\n"
            "node_grouped\ngather_roots\npass_fixed_kernel\nopenings_kernel\nbitfield_unpack_kernel\n"
            "unpack_range_kernel\nabsorb_kernel\npass_fixed_grouped\nnode_coop_kernel\ntree_tail_kernel\n"
@@ -587,11 +587,17 @@ extern "C" void free_device_buffers(void *d_buffers)
     delete b;
 }
 
-static void harvest(Slot &s)
+// A commit that failed on the device is reported on the buffers object (and its root left zero).
+static void harvest(CommitBuffers *b, Slot &s)
 {
     if (!s.busy) return;
-    cudaEventSynchronize(s.end);
-    if (s.user_root) memcpy(s.user_root, s.h_root, 32);
+    const cudaError_t e = cudaEventSynchronize(s.end);
+    if (e == cudaSuccess) {
+        if (s.user_root) memcpy(s.user_root, s.h_root, 32);
+    } else {
+        b->error = cuda_err(e, "commit on the device");
+        if (s.user_root) memset(s.user_root, 0, 32);
+    }
     s.busy = false;
 }
 
@@ -608,7 +614,7 @@ extern "C" uint64_t gen_device_streams(void *d_buffers, uint64_t n_streams, uint
     std::lock_guard<std::mutex> lk(b->mu);
     cudaSetDevice(b->device);
     if (merkleTreeArity) b->arity = (uint32_t)merkleTreeArity;
-    for (auto &s : b->slots) harvest(s);
+    for (auto &s : b->slots) harvest(b, s);
     b->last_end = nullptr;  // every slot is idle; slots may be destroyed below
     while (b->slots.size() > n_streams) {
         slot_destroy(b->slots.back());
@@ -707,10 +713,7 @@ static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_
         CK(cudaStreamWaitEvent(s.stream, s.blocks[k], 0), "block landed");
         {
             prof::Scope ps(prof::TRANSPOSE, s.stream);
-            dim3 grid((unsigned)((N + 31) / 32), (unsigned)((cb + 31) / 32));
-            ntt::transpose_kernel<<<grid, dim3(32, 8), 0, s.stream>>>(s.d_cm1 + c0 * N, staging + c0 * N, N, cb, N);
-            prof::count();
-            CK(cudaGetLastError(), "transpose");
+            CK(ntt::transpose(s.d_cm1 + c0 * N, staging + c0 * N, N, cb, N, s.stream), "transpose");
         }
         CK(ntt::lde(s.d_lde + c0 * NExt, s.d_cm1 + c0 * N, false, (uint32_t)nBits, (uint32_t)nBitsExt, cb,
                     s.d_scratch + c0 * N, s.stream),
@@ -798,7 +801,7 @@ extern "C" uint64_t commit_witness(void *pSetupCtx, void *params, uint64_t insta
         pick = 0;
         for (size_t i = 1; i < b->slots.size(); i++)
             if (b->slots[i].seq < b->slots[pick].seq) pick = i;
-        harvest(b->slots[pick]);
+        harvest(b, b->slots[pick]);
     }
     Slot &s = b->slots[pick];
     rc = slot_commit(b, s, sp->trace, si->nBits, si->nBitsExt, nCols, arity, lay);
@@ -831,7 +834,7 @@ extern "C" void get_stream_proofs(void *d_buffers)
     auto *b = (CommitBuffers *)d_buffers;
     if (!b) return;
     std::lock_guard<std::mutex> lk(b->mu);
-    for (auto &s : b->slots) harvest(s);
+    for (auto &s : b->slots) harvest(b, s);
 }
 
 extern "C" void get_stream_proofs_non_blocking(void *d_buffers)
@@ -840,7 +843,7 @@ extern "C" void get_stream_proofs_non_blocking(void *d_buffers)
     if (!b) return;
     std::lock_guard<std::mutex> lk(b->mu);
     for (auto &s : b->slots)
-        if (s.busy && cudaEventQuery(s.end) == cudaSuccess) harvest(s);
+        if (s.busy && cudaEventQuery(s.end) != cudaErrorNotReady) harvest(b, s);
 }
 
 extern "C" uint32_t register_host_memory(void *ptr, uint64_t size)
@@ -905,7 +908,7 @@ extern "C" void write_custom_commit(void *root, uint64_t arity, uint64_t nBits, 
         std::lock_guard<std::mutex> lk(b->mu);
         cudaSetDevice(b->device);
         Slot &s = b->slots[0];
-        harvest(s);
+        harvest(b, s);
         const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
         const uint64_t tsz = merkle::tree_num_elements(NExt, arity);
         rc = slot_commit(b, s, (const uint64_t *)buffer, nBits, nBitsExt, nCols, arity,
@@ -1003,6 +1006,18 @@ extern "C" const char *b200_timing_name(int category)
     return (category >= 0 && category < prof::NCAT) ? prof::kCatNames[category] : "";
 }
 extern "C" uint64_t b200_launch_count(void) { return prof::g_launches.load(); }
+
+extern "C" int b200_set_transpose_tma(int on) { return ntt::transpose_tma_enabled().exchange(on ? 1 : 0); }
+
+// the TMA transposes' error flag on the current device (1: a tile copy did not land within the
+// kernel's wait bound), reset to 0
+extern "C" int b200_tma_wait_errors(void)
+{
+    int v = 0, zero = 0;
+    if (cudaMemcpyFromSymbol(&v, g_tma_error, sizeof(int)) != cudaSuccess) return cuda_err(cudaGetLastError(), "flag");
+    CK(cudaMemcpyToSymbol(g_tma_error, &zero, sizeof(int)), "flag reset");
+    return v;
+}
 
 __global__ void __launch_bounds__(256) imad_probe_kernel(uint32_t *out, uint64_t iters, uint32_t seed)
 {

@@ -1,18 +1,35 @@
-// Commit server: a request loop with continuous admission (included at the end of pil2_b200.cu).
+// Commit server: a request loop with continuous batching (included at the end of pil2_b200.cu).
 //
-// Requests (host row-major traces) arrive at any time.  A worker thread admits them in arrival
-// order whenever a stream slot is free and the device-memory budget holds the request's buffers
-// (trace, scratch, LDE, tree); each admitted request runs H2D -> LDE -> tree -> root D2H on its own
-// stream, so requests admitted while others are on the GPU overlap with them.  Completion is
-// observed through an event; the LDE and the tree stay resident on the device (for later query
-// reads) until the caller releases the request.  Device buffers come from the stream-ordered pool
-// (cudaMallocAsync), which keeps freed memory cached for the next admissions.  No call blocks on
-// the GPU except b200_server_wait_all, whose wait is bounded by its timeout.
+// Requests (host row-major traces) arrive at any time.  A worker thread admits them whenever a
+// slot is free and the device-memory budget holds the request's buffers (trace, scratch, LDE,
+// tree), and turns them into units of work:
+//   * the small requests waiting together (LDE of at most `small_elems` elements each) become one
+//     batched unit: one batch::Plan over all of them, so their transposes, NTT windows, leaf sponge
+//     and tree levels run as shared grouped launches and a persistent leaf kernel;
+//   * a larger request is a plain unit: the single-instance commit.
+// Units are admitted while earlier ones run: each unit's host-to-device copy overlaps the kernels
+// of the units ahead of it, and each unit's kernels follow the previous unit's on the device.
+// Measured on a B200 with the C3 size mix, letting the units' kernels interleave instead (streams
+// of different priorities, no ordering) doubled the median latency at 5 requests/s and lowered the
+// throughput at 20 requests/s by 7 %: every kernel here fills the GPU, and co-resident commits only
+// slow each other down.  Small requests may overtake waiting large ones — a batched unit is
+// admitted ahead of the queue head — but a request is overtaken at most `max_overtakes` times, so
+// none waits forever.  Completion is observed through an event per unit; the LDE and the tree of
+// every request stay resident on the device (for later query reads) until the caller releases the
+// request.  Device buffers come from the server's own stream-ordered memory pool
+// (cudaMemPoolCreate), which keeps freed blocks cached for the next admissions without changing
+// the device's default pool.  No call blocks on the GPU except b200_server_wait_all, whose wait is
+// bounded by its timeout, and the pool trim of an admission that does not fit the cached blocks.
+//
+// Mode 0 (b200_server_configure) is the plain FIFO: every request a plain unit in arrival order;
+// kept as the comparison point.
 #pragma once
 #include <chrono>
 #include <condition_variable>
 #include <deque>
 #include <unordered_map>
+
+#include "batch.cuh"
 
 namespace serve {
 
@@ -29,48 +46,84 @@ struct Request {
     uint64_t *root_out = nullptr;
     uint64_t words_trace = 0, words_lde = 0, words_tree = 0;
     uint64_t *d_trace = nullptr, *d_scratch = nullptr, *d_lde = nullptr, *d_tree = nullptr;
-    uint64_t *h_root = nullptr;  // pinned 4 words
-    cudaEvent_t done = nullptr;
-    int slot = -1;
+    uint64_t root[4] = {0, 0, 0, 0};
     int status = 0;  // 0 queued, 1 running, 2 done, < 0 error
     bool released = false;
+    cudaStream_t stream = nullptr;  // the stream its buffers were last used on
     double t_submit = 0, t_admit = 0, t_done = 0;
+    uint32_t overtaken = 0;  // times a batch of smaller requests was admitted ahead of it
     std::string err;  // reason of a failed request (reported to the caller by status())
     uint64_t bytes() const { return 8 * (2 * words_trace + words_lde + words_tree); }
+    uint64_t elems() const { return (uint64_t)nCols << nBitsExt; }
 };
+
+// One admitted unit of work on one slot: a plain request or a batch of small ones.
+struct Unit {
+    std::vector<Request *> reqs;
+    bool batched = false;
+    int slot = -1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    batch::Plan *plan = nullptr;
+    unsigned char *d_table = nullptr;  // batched: the plan's device tables (from the pool)
+};
+
+constexpr size_t STAGING_BYTES = 1u << 20;  // per slot: a batched unit's tables and roots (pinned)
 
 class Server {
   public:
-    int device = 0;
+    int device = 0, sms = 148;
     uint64_t budget = 0, used = 0;
-    std::vector<cudaStream_t> streams;
+    int mode = 1;                          // 1 continuous batching, 0 FIFO
+    uint64_t small_elems = 1ull << 26;     // batched when NExt * nCols is at most this
+    uint32_t max_batch = 64;               // requests per batched unit
+    uint32_t max_overtakes = 4;            // times a waiting request may be overtaken by a batch
+    std::vector<cudaStream_t> streams;     // [slot]
+    std::vector<unsigned char *> staging;            // [slot] pinned
+    std::vector<uint64_t *> h_roots;                 // [slot] pinned, plain units' root
     std::vector<int> slot_busy;
     std::mutex mu;
     std::condition_variable cv;
     std::deque<Request *> queue;
-    std::vector<Request *> running;
+    std::vector<Unit *> running;
     std::unordered_map<int64_t, Request *> all;
     int64_t next_id = 1;
-    bool stop = false;
+    bool stop = false, configured = false;
     std::thread worker;
     cudaMemPool_t pool = nullptr;
-    cudaEvent_t last_done = nullptr;  // completion event of the most recently admitted request
+    cudaEvent_t last_done = nullptr;  // mode 0: completion of the most recently admitted unit
+    std::vector<cudaEvent_t> spare_events;
     int family = 2;                   // hash family of this server's commits (fixed at creation)
+    uint64_t units_plain = 0, units_batched = 0, batched_requests = 0, pool_trims = 0, overtakes = 0;
+    double t_start = 0;
 
     int start(int dev, uint64_t budget_bytes, uint32_t slots)
     {
         device = dev;
         budget = budget_bytes;
+        t_start = now_ms();
         CK(cudaSetDevice(dev), "cudaSetDevice");
         int rc = ensure_init_current();
         if (rc) return rc;
-        CK(cudaDeviceGetDefaultMemPool(&pool, dev), "mem pool");
-        uint64_t keep = UINT64_MAX;  // keep freed blocks cached in the pool
+        if ((rc = batch_kernel_attrs())) return rc;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        CK(cudaMemPoolCreate(&pool, &props), "server memory pool");
+        uint64_t keep = UINT64_MAX;  // keep freed blocks cached in this pool
         CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "mem pool threshold");
         for (uint32_t i = 0; i < slots; i++) {
             cudaStream_t s;
             CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
             streams.push_back(s);
+            unsigned char *st = nullptr;
+            uint64_t *hr = nullptr;
+            CK(cudaMallocHost((void **)&st, STAGING_BYTES), "pinned staging");
+            staging.push_back(st);
+            CK(cudaMallocHost((void **)&hr, 32), "pinned root");
+            h_roots.push_back(hr);
             slot_busy.push_back(0);
         }
         worker = std::thread([this] { loop(); });
@@ -86,27 +139,30 @@ class Server {
         cv.notify_all();
         if (worker.joinable()) worker.join();
         cudaSetDevice(device);
+        for (cudaStream_t s : streams) cudaStreamSynchronize(s);
+        for (Unit *u : running) finish_unit(u, cudaEventQuery(u->done) == cudaSuccess);
         for (auto &kv : all) {
             Request *r = kv.second;
-            if (r->done) cudaEventSynchronize(r->done);
             free_buffers(r, nullptr);
-            if (r->done) cudaEventDestroy(r->done);
-            if (r->h_root) cudaFreeHost(r->h_root);
             delete r;
         }
-        for (cudaStream_t s : streams) {
-            cudaStreamSynchronize(s);
-            cudaStreamDestroy(s);
-        }
+        cudaDeviceSynchronize();
+        for (cudaStream_t s : streams) cudaStreamDestroy(s);
+        for (unsigned char *p : staging) cudaFreeHost(p);
+        for (uint64_t *p : h_roots) cudaFreeHost(p);
+        for (cudaEvent_t e : spare_events) cudaEventDestroy(e);
+        if (pool) cudaMemPoolDestroy(pool);
     }
 
+    // the two blocks of a request (d_scratch and d_tree point into them)
     void free_buffers(Request *r, cudaStream_t s)
     {
-        for (uint64_t **p : {&r->d_trace, &r->d_scratch, &r->d_lde, &r->d_tree})
+        for (uint64_t **p : {&r->d_trace, &r->d_lde})
             if (*p) {
                 cudaFreeAsync(*p, s);
                 *p = nullptr;
             }
+        r->d_scratch = r->d_tree = nullptr;
     }
 
     int64_t submit(const uint64_t *trace, uint32_t nBits, uint32_t nBitsExt, uint32_t nCols, uint32_t arity,
@@ -132,104 +188,252 @@ class Server {
             r->id = next_id++;
             all[r->id] = r;
             queue.push_back(r);
+            configured = true;
         }
         cv.notify_all();
         return r->id;
     }
 
-    // all four device buffers of a request, or none
+    cudaError_t pool_alloc(uint64_t **p, uint64_t words, cudaStream_t s)
+    {
+        return cudaMallocFromPoolAsync((void **)p, 8 * (words ? words : 1), pool, s);
+    }
+
+    // A request's buffers as two pool blocks, or none: [trace | scratch], released behind its
+    // kernels, and [LDE | tree], kept until the request is released (fewer, larger blocks keep the
+    // pool's cache less fragmented than one block per buffer).
     bool alloc_request(Request *r, cudaStream_t s)
     {
-        if (cudaMallocAsync((void **)&r->d_trace, 8 * (r->words_trace ? r->words_trace : 1), s) == cudaSuccess &&
-            cudaMallocAsync((void **)&r->d_scratch, 8 * (r->words_trace ? r->words_trace : 1), s) == cudaSuccess &&
-            cudaMallocAsync((void **)&r->d_lde, 8 * (r->words_lde ? r->words_lde : 1), s) == cudaSuccess &&
-            cudaMallocAsync((void **)&r->d_tree, 8 * r->words_tree, s) == cudaSuccess)
+        const uint64_t w1 = 2 * r->words_trace, w2 = r->words_lde + r->words_tree;
+        if (pool_alloc(&r->d_trace, w1, s) == cudaSuccess && pool_alloc(&r->d_lde, w2, s) == cudaSuccess) {
+            r->d_scratch = r->d_trace + r->words_trace;
+            r->d_tree = r->d_lde + r->words_lde;
             return true;
+        }
         cudaGetLastError();
         free_buffers(r, s);
         return false;
     }
 
-    // admit the head of the queue onto a free slot; caller holds mu
-    bool admit_one()
+    // Buffers of every request of a unit; when the cached blocks do not fit, the pool is trimmed
+    // (after the running units' frees have executed) and the allocation retried once.
+    bool alloc_unit(Unit *u)
     {
-        if (queue.empty()) return false;
-        Request *r = queue.front();
-        int slot = -1;
-        for (size_t i = 0; i < streams.size(); i++)
-            if (!slot_busy[i]) {
-                slot = (int)i;
-                break;
-            }
-        if (slot < 0 || used + r->bytes() > budget) return false;
-        queue.pop_front();
-        cudaStream_t s = streams[slot];
-        r->slot = slot;
-        r->t_admit = now_ms();
-        int rc = B200_OK;
-        if (!r->h_root && cudaMallocHost((void **)&r->h_root, 32) != cudaSuccess) rc = B200_ENOMEM;
-        if (!rc && !r->done && cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming) != cudaSuccess)
-            rc = B200_ECUDA;
-        if (!rc && !alloc_request(r, s)) {
-            // The pool keeps freed blocks cached; when the cached sizes do not fit this request,
-            // return them to the device (after the running requests' frees have executed) and retry.
-            for (cudaStream_t t : streams) cudaStreamSynchronize(t);
-            cudaMemPoolTrimTo(pool, 0);
-            cudaGetLastError();
-            if (!alloc_request(r, s)) {
-                rc = B200_ENOMEM;
-                r->err = "device buffers for the request could not be allocated";
+        for (int attempt = 0; attempt < 2; attempt++) {
+            bool ok = true;
+            for (Request *r : u->reqs)
+                if (!alloc_request(r, u->stream)) {
+                    ok = false;
+                    break;
+                }
+            if (ok) return true;
+            for (Request *r : u->reqs) free_buffers(r, u->stream);
+            if (attempt == 0) {
+                for (cudaStream_t t : streams) cudaStreamSynchronize(t);
+                cudaMemPoolTrimTo(pool, 0);
+                pool_trims++;
+                cudaGetLastError();
             }
         }
-        if (!rc && r->words_trace &&
-            cudaMemcpyAsync(r->d_trace, r->trace, 8 * r->words_trace, cudaMemcpyHostToDevice, s) != cudaSuccess)
-            rc = B200_ECUDA;
-        // kernels of admitted requests run in admission order (the H2D above overlaps the previous
-        // request's kernels); interleaved requests would each take longer and finish together
-        if (!rc && last_done) cudaStreamWaitEvent(s, last_done, 0);
-        if (!rc) rc = commit_device_fam(nullptr, r->d_lde, r->d_tree, r->d_trace, 1, r->nBits, r->nBitsExt, r->nCols,
-                                        r->arity, r->d_scratch, s, family);
-        if (!rc && cudaMemcpyAsync(r->h_root, r->d_tree + r->words_tree - 4, 32, cudaMemcpyDeviceToHost, s) !=
-                       cudaSuccess)
-            rc = B200_ECUDA;
-        if (!rc) {
-            // the trace copy and the scratch are not needed once the commit has run
+        return false;
+    }
+
+    cudaEvent_t take_event()
+    {
+        if (!spare_events.empty()) {
+            cudaEvent_t e = spare_events.back();
+            spare_events.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+        return e;
+    }
+
+    // Enqueue a unit's copies and kernels on its stream; returns 0 or a B200 error code.
+    int launch_unit(Unit *u)
+    {
+        cudaStream_t s = u->stream;
+        if (!alloc_unit(u)) {
+            for (Request *r : u->reqs) r->err = "device buffers for the request could not be allocated";
+            return B200_ENOMEM;
+        }
+        for (Request *r : u->reqs) {
+            r->stream = s;
+            if (r->words_trace &&
+                cudaMemcpyAsync(r->d_trace, r->trace, 8 * r->words_trace, cudaMemcpyHostToDevice, s) != cudaSuccess)
+                return B200_ECUDA;
+        }
+        // kernels in admission order (the copies above overlap the units ahead)
+        if (last_done && cudaStreamWaitEvent(s, last_done, 0) != cudaSuccess) return B200_ECUDA;
+        if (!u->batched) {
+            Request *r = u->reqs[0];
+            int rc = commit_device_fam(nullptr, r->d_lde, r->d_tree, r->d_trace, 1, r->nBits, r->nBitsExt, r->nCols,
+                                       r->arity, r->d_scratch, s, family);
+            if (rc) return rc;
+            if (cudaMemcpyAsync(h_roots[u->slot], r->d_tree + r->words_tree - 4, 32, cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess)
+                return B200_ECUDA;
+        } else {
+            std::vector<batch::Inst> in;
+            for (Request *r : u->reqs)
+                in.push_back(batch::Inst{r->d_trace, r->d_scratch, r->d_lde, r->d_tree, r->nBits, r->nBitsExt,
+                                         r->nCols, r->arity});
+            u->plan = new batch::Plan();
+            u->plan->borrowed = true;
+            if (!u->plan->build(in, sms, family)) return set_err(B200_EINVAL, "batched unit: unsupported shape");
+            const size_t tbytes = (u->plan->table.size() + 255) & ~size_t(255);
+            if (tbytes + 32 * (u->reqs.size() + 1) > STAGING_BYTES)
+                return set_err(B200_EINVAL, "batched unit: descriptor tables above the staging size");
+            unsigned char *st = staging[u->slot];
+            memcpy(st, u->plan->table.data(), u->plan->table.size());
+            if (cudaMallocFromPoolAsync((void **)&u->d_table, tbytes, pool, s) != cudaSuccess) {
+                cudaGetLastError();
+                return B200_ENOMEM;
+            }
+            if (cudaMemcpyAsync(u->d_table, st, u->plan->table.size(), cudaMemcpyHostToDevice, s) != cudaSuccess)
+                return B200_ECUDA;
+            u->plan->d_table = u->d_table;
+            u->plan->h_roots = (uint64_t *)(st + tbytes);
+            if (u->plan->enqueue(s) != cudaSuccess) return B200_ECUDA;
+        }
+        // the trace copy and the scratch are not needed once the commit has run
+        for (Request *r : u->reqs) {
             cudaFreeAsync(r->d_trace, s);
-            cudaFreeAsync(r->d_scratch, s);
             r->d_trace = r->d_scratch = nullptr;
-            if (cudaEventRecord(r->done, s) != cudaSuccess) rc = B200_ECUDA;
-            else last_done = r->done;
         }
-        if (rc) {
-            free_buffers(r, s);
-            if (r->err.empty()) r->err = "request failed on the device (CUDA error)";
-            r->status = rc;
-            r->t_done = now_ms();
-            return true;
+        if (!(u->done = take_event()) || cudaEventRecord(u->done, s) != cudaSuccess) return B200_ECUDA;
+        last_done = u->done;
+        return B200_OK;
+    }
+
+    int free_slot() const
+    {
+        for (size_t i = 0; i < slot_busy.size(); i++)
+            if (!slot_busy[i]) return (int)i;
+        return -1;
+    }
+
+    // One admission round (caller holds mu): while a slot is free, the next unit holds the waiting
+    // small requests (in arrival order, up to max_batch; a batch when there are several), passing
+    // the large requests between them unless one of those has been overtaken max_overtakes times;
+    // with no small request waiting, the queue head.  Stops at the first unit the budget cannot hold.
+    void admit()
+    {
+        while (!queue.empty()) {
+            const int slot = free_slot();
+            if (slot < 0) return;
+            auto *u = new Unit();
+            u->slot = slot;
+            uint64_t add = 0;
+            if (mode == 1) {
+                std::vector<size_t> small;
+                for (size_t i = 0; i < queue.size() && small.size() < max_batch; i++) {
+                    Request *r = queue[i];
+                    if (r->elems() <= small_elems) {
+                        if (used + add + r->bytes() > budget) break;
+                        small.push_back(i);
+                        add += r->bytes();
+                    } else if (r->overtaken >= max_overtakes) {
+                        break;  // this one goes next: nothing behind it passes it again
+                    }
+                }
+                if (!small.empty()) {
+                    for (size_t i = 0; i < small.back(); i++)
+                        if (queue[i]->elems() > small_elems) {
+                            queue[i]->overtaken++;
+                            overtakes++;
+                        }
+                    for (size_t k = small.size(); k-- > 0;) {
+                        u->reqs.insert(u->reqs.begin(), queue[small[k]]);
+                        queue.erase(queue.begin() + (std::ptrdiff_t)small[k]);
+                    }
+                } else {
+                    add = 0;
+                }
+            }
+            if (u->reqs.empty()) {
+                Request *head = queue.front();
+                if (used + head->bytes() > budget) {
+                    delete u;
+                    return;
+                }
+                queue.pop_front();
+                add = head->bytes();
+                u->reqs.push_back(head);
+            }
+            u->batched = u->reqs.size() > 1;
+            u->stream = streams[slot];
+            const double t = now_ms();
+            for (Request *r : u->reqs) r->t_admit = t;
+            int rc = launch_unit(u);
+            if (rc) {
+                for (Request *r : u->reqs) {
+                    free_buffers(r, u->stream);
+                    if (r->err.empty()) r->err = "request failed on the device (CUDA error)";
+                    r->status = rc;
+                    r->t_done = now_ms();
+                }
+                if (u->d_table) cudaFreeAsync(u->d_table, u->stream);
+                if (u->done) spare_events.push_back(u->done);
+                delete u->plan;
+                delete u;
+                continue;
+            }
+            used += add;
+            slot_busy[slot] = 1;
+            for (Request *r : u->reqs) r->status = 1;
+            if (u->batched) {
+                units_batched++;
+                batched_requests += u->reqs.size();
+            } else {
+                units_plain++;
+            }
+            running.push_back(u);
         }
-        used += r->bytes();
-        slot_busy[slot] = 1;
-        r->status = 1;
-        running.push_back(r);
-        return true;
+    }
+
+    // results of a finished unit to its requests; frees the unit (caller holds mu)
+    void finish_unit(Unit *u, bool ok)
+    {
+        const double t = now_ms();
+        for (size_t i = 0; i < u->reqs.size(); i++) {
+            Request *r = u->reqs[i];
+            r->t_done = t;
+            if (ok) {
+                const uint64_t *src = u->batched ? u->plan->h_roots + 4 * i : h_roots[u->slot];
+                memcpy(r->root, src, 32);
+                if (r->root_out) memcpy(r->root_out, r->root, 32);
+                r->status = 2;
+                used -= 8 * 2 * r->words_trace;  // trace + scratch were freed behind the kernels
+            } else {
+                r->status = B200_ECUDA;
+                r->err = "request failed on the device (CUDA error)";
+                free_buffers(r, u->stream);
+                used -= r->bytes();
+            }
+        }
+        if (u->d_table) cudaFreeAsync(u->d_table, u->stream);
+        if (u->done) spare_events.push_back(u->done);
+        if (last_done == u->done) last_done = nullptr;
+        slot_busy[u->slot] = 0;
+        delete u->plan;
+        delete u;
     }
 
     // caller holds mu
     void harvest()
     {
         for (size_t i = 0; i < running.size();) {
-            Request *r = running[i];
-            if (cudaEventQuery(r->done) == cudaSuccess) {
-                r->t_done = now_ms();
-                if (r->root_out) memcpy(r->root_out, r->h_root, 32);
-                r->status = 2;
-                slot_busy[r->slot] = 0;
-                used -= 8 * 2 * r->words_trace;  // trace + scratch were freed at admission
-                running[i] = running.back();
-                running.pop_back();
-            } else {
+            Unit *u = running[i];
+            const cudaError_t q = cudaEventQuery(u->done);
+            if (q == cudaErrorNotReady) {
                 i++;
+                continue;
             }
+            running[i] = running.back();
+            running.pop_back();
+            finish_unit(u, q == cudaSuccess);
         }
     }
 
@@ -239,8 +443,7 @@ class Server {
         std::unique_lock<std::mutex> lk(mu);
         while (!stop) {
             harvest();
-            while (admit_one()) {
-            }
+            admit();
             cv.notify_all();
             cv.wait_for(lk, std::chrono::microseconds(running.empty() ? 2000 : 50));
         }
@@ -280,7 +483,7 @@ class Server {
         if (r->status != 2 && r->status >= 0) return set_err(B200_EBUSY, "request still in flight");
         if (!r->released) {
             cudaSetDevice(device);
-            free_buffers(r, streams[r->slot >= 0 ? r->slot : 0]);
+            free_buffers(r, r->stream);
             if (r->status == 2) used -= 8 * (r->words_lde + r->words_tree);
             r->released = true;
         }
@@ -305,6 +508,47 @@ extern "C" void *b200_server_new(int device, uint64_t budget_bytes, uint32_t slo
         return nullptr;
     }
     return s;
+}
+
+extern "C" int b200_server_configure(void *srv, int batching, uint64_t small_elems, uint32_t max_batch)
+{
+    auto *s = (serve::Server *)srv;
+    if (!s) return set_err(B200_EINVAL, "null server");
+    if (batching != 0 && batching != 1) return set_err(B200_EINVAL, "batching must be 0 (FIFO) or 1");
+    if (max_batch == 0 || max_batch > 1024) return set_err(B200_EINVAL, "max_batch must be 1..1024");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->configured) return set_err(B200_EBUSY, "b200_server_configure: requests already submitted");
+    s->mode = batching;
+    s->small_elems = small_elems;
+    s->max_batch = max_batch;
+    return B200_OK;
+}
+
+// counters, in this order: plain units, batched units, requests in batched units, pool trims (an
+// admission that did not fit the pool's cached blocks), times a waiting request was passed
+extern "C" int b200_server_stats(void *srv, uint64_t *out, uint64_t n)
+{
+    auto *s = (serve::Server *)srv;
+    if (!s || (n && !out)) return set_err(B200_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    const uint64_t v[5] = {s->units_plain, s->units_batched, s->batched_requests, s->pool_trims, s->overtakes};
+    for (uint64_t i = 0; i < n && i < 5; i++) out[i] = v[i];
+    return B200_OK;
+}
+
+// submission, admission and completion time of a request, ms since the server was created
+extern "C" int b200_server_request_times(void *srv, int64_t id, double *times3)
+{
+    auto *s = (serve::Server *)srv;
+    if (!s || !times3) return set_err(B200_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return set_err(B200_EINVAL, "unknown request id");
+    const serve::Request *r = it->second;
+    times3[0] = r->t_submit - s->t_start;
+    times3[1] = r->t_admit ? r->t_admit - s->t_start : -1;
+    times3[2] = r->t_done ? r->t_done - s->t_start : -1;
+    return B200_OK;
 }
 
 extern "C" int64_t b200_server_submit(void *srv, const uint64_t *host_trace, uint64_t nBits, uint64_t nBitsExt,

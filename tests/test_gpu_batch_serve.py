@@ -135,15 +135,20 @@ def test_one_shot_batch_entry(pkg, torch_cuda):
         assert (roots[j] == r).all()
 
 
-def test_server_alone_equals_in_the_mix(pkg, torch_cuda):
-    """Each request's root is the same served alone and served among overlapping requests."""
+@pytest.mark.parametrize("mode,small", [(1, 1 << 26), (1, 1 << 17), (0, 1 << 26)])
+def test_server_alone_equals_in_the_mix(pkg, torch_cuda, mode, small):
+    """Each request's root is the same served alone and served among overlapping requests: with
+    continuous batching (small requests admitted together share one batched unit; with the lower
+    threshold the larger ones run as plain units beside them) and in FIFO mode."""
     lib = pkg.load()
-    shapes = [(12, 13, 40, 4), (14, 15, 9, 4), (10, 12, 100, 3), (15, 16, 30, 4), (9, 10, 5, 2), (13, 14, 64, 4)]
+    shapes = [(12, 13, 40, 4), (14, 15, 9, 4), (10, 12, 100, 3), (15, 16, 30, 4), (9, 10, 5, 2), (13, 14, 64, 4),
+              (16, 17, 24, 4)]
     traces = [oracle.random_field((1 << nb, nc), 42 + i) for i, (nb, nbe, nc, ar) in enumerate(shapes)]
     alone = [pkg.commit_host(tr, nbe, ar)[0] for tr, (nb, nbe, nc, ar) in zip(traces, shapes)]
     srv = lib.b200_server_new(0, 8 << 30, 4)
     assert srv, lib.b200_last_error()
     try:
+        assert lib.b200_server_configure(srv, mode, small, 64) == 0, lib.b200_last_error()
         ids, outs = [], []
         for rep in range(3):  # all requests in flight together, three times over
             for i, (nb, nbe, nc, ar) in enumerate(shapes):
@@ -166,6 +171,38 @@ def test_server_alone_equals_in_the_mix(pkg, torch_cuda):
             assert lib.b200_server_release(srv, rid) == 0
         # an oversized request is refused, not queued forever
         assert lib.b200_server_submit(srv, traces[0].ctypes.data, 24, 26, 64, 4, None) == pkg.B200_EBUSY
+        st = (ctypes.c_uint64 * 5)()
+        assert lib.b200_server_stats(srv, st, 5) == 0
+        plain, batched, in_batches = st[0], st[1], st[2]
+        assert plain + in_batches == 3 * len(shapes)
+        if mode == 0:
+            assert batched == 0
+        # configuring after the first submit is refused
+        assert lib.b200_server_configure(srv, 1, 1 << 20, 8) == pkg.B200_EBUSY
+    finally:
+        lib.b200_server_free(srv)
+
+
+def test_server_batches_small_requests(pkg, torch_cuda):
+    """Requests queued together while the server is busy are admitted as one batched unit."""
+    lib = pkg.load()
+    nb, nbe, nc = 11, 12, 20
+    traces = [oracle.random_field((1 << nb, nc), 70 + i) for i in range(12)]
+    want = [oracle.Oracle().commit(t, nbe, 4)[0] for t in traces]
+    srv = lib.b200_server_new(0, 4 << 30, 1)  # one slot: the first request runs, the rest queue
+    assert srv
+    try:
+        outs, ids = [], []
+        for t in traces:
+            out = np.zeros(4, dtype=np.uint64)
+            ids.append(lib.b200_server_submit(srv, t.ctypes.data, nb, nbe, nc, 4, out.ctypes.data))
+            outs.append(out)
+        assert lib.b200_server_wait_all(srv, 60000) == 0, lib.b200_last_error()
+        for out, w in zip(outs, want):
+            assert (out == w).all()
+        st = (ctypes.c_uint64 * 5)()
+        lib.b200_server_stats(srv, st, 5)
+        assert st[1] >= 1 and st[2] >= 2, list(st)
     finally:
         lib.b200_server_free(srv)
 
