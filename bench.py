@@ -891,7 +891,7 @@ def main():
     ap.add_argument("--rates", default="5,20,80", help="c5: Poisson arrival rates per second")
     ap.add_argument("--duration", type=float, default=60.0, help="c5: seconds of arrivals per rate")
     ap.add_argument("--pool", type=int, default=12, help="c5: distinct C3-distributed request shapes")
-    ap.add_argument("--slots", type=int, default=2, help="c5: server slots (units admitted at once)")
+    ap.add_argument("--slots", type=int, default=4, help="c5: server slots (units admitted at once)")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0, help="c5: server device-memory budget")
     ap.add_argument("--serve-timeout", type=float, default=1800.0, help="c5: give up after this many seconds")
     ap.add_argument("--no-legs", action="store_true",
