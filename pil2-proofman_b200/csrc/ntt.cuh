@@ -374,35 +374,172 @@ __device__ __forceinline__ void phases_fixed(uint64_t *sm)
     }
 }
 
+constexpr int log2_const(int x) { return x <= 1 ? 0 : 1 + log2_const(x >> 1); }
+
+// Thread / iteration decomposition of a fixed-shape tile.  Element q = threadIdx.x + it * NT of the
+// tile is (mid, lane) = (q >> LGL, q & Lm).  When NT is a multiple of 2^LGL (SPLIT) a thread keeps
+// one lane, and mid = M0 + it * 2^MB with M0 = threadIdx.x >> LGL below 2^MB: the low MB bits of
+// mid come from the thread, the high LOG_IT bits from the iteration, so
+//   brev_K(mid) = (brev_MB(M0) << LOG_IT) + brev_LOG_IT(it).
+// Any factor w^(brev_K(mid) * c) is then a per-thread constant times a power of w^c whose exponent
+// is brev_LOG_IT(it): visiting the iterations in bit-reversed order makes that exponent count up,
+// and the factors are running products (no table lookups in the loop).
+template <int K, int LGL>
+struct Iter {
+    static constexpr int T = Shape<K, LGL>::T, NT = Shape<K, LGL>::NT, IT = (T + NT - 1) / NT;
+    static constexpr int LOG_NT = log2_const(NT);
+    static constexpr bool SPLIT = (T % NT == 0) && LOG_NT >= LGL && (1 << (K + LGL)) == T;
+    static constexpr int MB = SPLIT ? LOG_NT - LGL : 0;
+    static constexpr int LOG_IT = SPLIT ? K - MB : 0;
+    static constexpr int CH = IT < 4 ? IT : 4;  // independent product chains (latency)
+};
+
+// Running powers f(it') = A * B^it' for it' = 0 .. IT-1, as CH interleaved chains: chain c yields
+// it' = c, c + CH, c + 2 CH, ...  next(c) returns chain c's current value and advances it.
+template <int CH>
+struct Powers {
+    uint64_t v[CH];
+    uint64_t step;  // B^CH
+    __device__ __forceinline__ void init(uint64_t A, uint64_t B)
+    {
+        v[0] = A;
+#pragma unroll
+        for (int c = 1; c < CH; c++) v[c] = gl::mul(v[c - 1], B);
+        uint64_t s = B;
+#pragma unroll
+        for (int c = 1; c < CH; c++) s = gl::mul(s, B);  // B^CH (CH <= 4)
+        step = s;
+    }
+    __device__ __forceinline__ uint64_t next(int c)
+    {
+        const uint64_t r = v[c];
+        v[c] = gl::mul(v[c], step);
+        return r;
+    }
+};
+
+// The inter-window twiddles of this thread's elements, w_{2^(s0+K)}^(brev_K(mid) * lo) (SPLIT shapes).
+template <int K, int LGL>
+__device__ __forceinline__ void window_twiddles(Powers<Iter<K, LGL>::CH> &pw, uint32_t lob, uint32_t tw_shift, bool inv)
+{
+    using I = Iter<K, LGL>;
+    constexpr uint32_t Lm = (1u << LGL) - 1;
+    const uint32_t lo = (lob << LGL) | (threadIdx.x & Lm);
+    const uint32_t M0 = threadIdx.x >> LGL;
+    const uint32_t e0 = (brev_bits(M0, I::MB) << I::LOG_IT) * lo;  // < 2^(s0 + K) <= 2^26
+    pw.init(big_twiddle((uint64_t)e0 << tw_shift, inv), big_twiddle((uint64_t)lo << tw_shift, inv));
+}
+
 // Register-path tile load of a fixed-shape window: the gather (with the Q stage's source remap
-// and scale), the forward windows' inter-window twiddle, the store to shared memory.  ONE: the
-// twiddles are powers of w_8192 (s0 + K <= 13, the first forward window at blowup 2), so each is
-// one entry of the high table instead of a product of a low and a high entry.
-template <int K, int LGL, bool DIF, bool ONE>
+// and scale), the forward windows' inter-window twiddle, the store to shared memory.  With a SPLIT
+// shape the twiddles are running products (Iter); otherwise each is a product of two table entries.
+template <int K, int LGL, bool DIF>
 __device__ __forceinline__ void load_tile(uint64_t *sm, const Pass &a, const uint64_t *S, uint32_t base,
                                           uint32_t lob, uint32_t s0, uint32_t tw_shift)
 {
-    constexpr int T = Shape<K, LGL>::T, NT = Shape<K, LGL>::NT;
-    constexpr int IT = (T + NT - 1) / NT;
+    using I = Iter<K, LGL>;
+    constexpr int T = I::T, NT = I::NT, IT = I::IT;
     constexpr uint32_t Lm = (1u << LGL) - 1;
     const uint32_t rep = a.rep, gshift = a.gshift, goff = (uint32_t)a.goff;
-#pragma unroll 4  // full unrolling hoists all 16 loads of a thread and spills at 64 registers
-    for (int it = 0; it < IT; it++) {
-        const uint32_t q = threadIdx.x + (uint32_t)it * NT;
-        if ((T % NT) != 0 && q >= (uint32_t)T) break;
-        const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
-        uint64_t v = S[((pos >> rep) << gshift) + goff];
-        if (a.scale) v = gl::mul(v, a.scale);
-        if (!DIF && s0 > 0) {
-            const uint32_t lo = (lob << LGL) | (q & Lm);
-            const uint32_t E = (__brev(q >> LGL) >> (32 - K)) * lo;
-            if (ONE) {
-                if (E) v = gl::mul(v, __ldg(g_ntt_tw_hi_fwd + (E << (13 - s0 - K))));
-            } else if (E) {
-                v = gl::mul(v, big_twiddle((uint64_t)(E << tw_shift), false));
+    const bool tw = !DIF && s0 > 0;
+    if constexpr (I::SPLIT) {
+        Powers<I::CH> pw;
+        if (tw) window_twiddles<K, LGL>(pw, lob, tw_shift, false);
+#pragma unroll 1
+        for (int jj = 0; jj < IT; jj += I::CH) {
+#pragma unroll
+            for (int c = 0; c < I::CH; c++) {
+                const uint32_t it = brev_bits((uint32_t)(jj + c), I::LOG_IT);
+                const uint32_t q = threadIdx.x + it * NT;
+                const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
+                uint64_t v = S[((pos >> rep) << gshift) + goff];
+                if (a.scale) v = gl::mul(v, a.scale);
+                if (tw) v = gl::mul(v, pw.next(c));
+                sm[pad16(q)] = v;
             }
         }
-        sm[pad16(q)] = v;
+    } else {
+#pragma unroll 4  // full unrolling hoists all 16 loads of a thread and spills at 64 registers
+        for (int it = 0; it < IT; it++) {
+            const uint32_t q = threadIdx.x + (uint32_t)it * NT;
+            if ((T % NT) != 0 && q >= (uint32_t)T) break;
+            const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
+            uint64_t v = S[((pos >> rep) << gshift) + goff];
+            if (a.scale) v = gl::mul(v, a.scale);
+            if (tw) {
+                const uint32_t lo = (lob << LGL) | (q & Lm);
+                const uint32_t E = (__brev(q >> LGL) >> (32 - K)) * lo;
+                if (E) v = gl::mul(v, big_twiddle((uint64_t)(E << tw_shift), false));
+            }
+            sm[pad16(q)] = v;
+        }
+    }
+}
+
+// Tile store of a fixed-shape window: the inverse windows' inter-window twiddle or, in the last
+// inverse window (s0 = 0, LGL = 0), the coset scale 7^bitrev(pos) / N; canonical values after the
+// last forward window.
+template <int K, int LGL, bool DIF>
+__device__ __forceinline__ void store_tile(const uint64_t *sm, const Pass &a, uint64_t *D, uint32_t base, uint32_t lob,
+                                           uint32_t s0, uint32_t tw_shift)
+{
+    using I = Iter<K, LGL>;
+    constexpr int T = I::T, NT = I::NT, IT = I::IT;
+    constexpr uint32_t Lm = (1u << LGL) - 1;
+    const bool tw = DIF && s0 > 0;
+    const uint32_t post = a.post;
+    if constexpr (I::SPLIT) {
+        Powers<I::CH> pw;
+        if (tw) {
+            window_twiddles<K, LGL>(pw, lob, tw_shift, true);
+        } else if (post == POST_COSET) {
+            // pos = base | q (s0 = 0, LGL = 0), base = hi << K: brev_lg(pos) = brev_lg(base) +
+            // ((brev_MB(tid) << LOG_IT) + brev_LOG_IT(it)) << (lg - K)
+            const uint32_t lg = a.lg, up = lg - K;
+            const uint32_t e0 = brev_bits(base, lg) + ((brev_bits(threadIdx.x, I::MB) << I::LOG_IT) << up);
+            const uint64_t c0 =
+                gl::mul(__ldg(g_ntt_sh_lo_n + (lg << 12) + (e0 & 4095)), __ldg(g_ntt_sh_hi + (e0 >> 12)));
+            const uint32_t es = 1u << up;  // 7^(2^up), without the 1/N of the lg table (lg 0: 2^0)
+            const uint64_t st = gl::mul(__ldg(g_ntt_sh_lo_n + (es & 4095)), __ldg(g_ntt_sh_hi + (es >> 12)));
+            pw.init(c0, st);
+        }
+#pragma unroll 1
+        for (int jj = 0; jj < IT; jj += I::CH) {
+#pragma unroll
+            for (int c = 0; c < I::CH; c++) {
+                const uint32_t it = brev_bits((uint32_t)(jj + c), I::LOG_IT);
+                const uint32_t q = threadIdx.x + it * NT;
+                const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
+                uint64_t v = sm[pad16(q)];
+                if (tw || post == POST_COSET)
+                    v = gl::mul(v, pw.next(c));
+                else if (post == POST_CANON)
+                    v = gl::canon(v);
+                D[pos] = v;
+            }
+        }
+    } else {
+#pragma unroll 4  // full unrolling hoists all 16 loads of a thread and spills at 64 registers
+        for (int it = 0; it < IT; it++) {
+            const uint32_t q = threadIdx.x + (uint32_t)it * NT;
+            if ((T % NT) != 0 && q >= (uint32_t)T) break;
+            const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
+            uint64_t v = sm[pad16(q)];
+            if (tw) {
+                const uint32_t lo = (lob << LGL) | (q & Lm);
+                const uint32_t E = (__brev(q >> LGL) >> (32 - K)) * lo;
+                if (E) v = gl::mul(v, big_twiddle((uint64_t)(E << tw_shift), true));
+            }
+            if (post == POST_COSET) {
+                const uint32_t br = brev_bits(pos, a.lg);
+                const uint64_t f =
+                    gl::mul(__ldg(g_ntt_sh_lo_n + (a.lg << 12) + (br & 4095)), __ldg(g_ntt_sh_hi + (br >> 12)));
+                v = gl::mul(v, f);
+            } else if (post == POST_CANON) {
+                v = gl::canon(v);
+            }
+            D[pos] = v;
+        }
     }
 }
 
@@ -441,37 +578,15 @@ __device__ __forceinline__ void pass_fixed_body(const Pass &a, uint32_t tile, ui
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    } else if (!inv && s0 > 0 && s0 + K <= 13) {
-        load_tile<K, LGL, DIF, true>(sm, a, S, base, lob, s0, tw_shift);
     } else {
-        load_tile<K, LGL, DIF, false>(sm, a, S, base, lob, s0, tw_shift);
+        load_tile<K, LGL, DIF>(sm, a, S, base, lob, s0, tw_shift);
     }
     __syncthreads();
     if constexpr (inv)
         phases_fixed<true, K, LGL, K / NTT_PHASE_BITS>(sm);
     else
         phases_fixed<false, K, LGL, 0>(sm);
-#pragma unroll 4  // full unrolling hoists all 16 loads of a thread and spills at 64 registers
-    for (int it = 0; it < IT; it++) {
-        const uint32_t q = threadIdx.x + (uint32_t)it * NT;
-        if ((T % NT) != 0 && q >= (uint32_t)T) break;
-        const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
-        uint64_t v = sm[pad16(q)];
-        if (inv && s0 > 0) {
-            const uint32_t lo = (lob << LGL) | (q & Lm);
-            const uint32_t E = (__brev(q >> LGL) >> (32 - K)) * lo;
-            if (E) v = gl::mul(v, big_twiddle((uint64_t)(E << tw_shift), true));
-        }
-        if (a.post == POST_COSET) {
-            const uint32_t br = brev_bits(pos, a.lg);
-            const uint64_t f =
-                gl::mul(__ldg(g_ntt_sh_lo_n + (a.lg << 12) + (br & 4095)), __ldg(g_ntt_sh_hi + (br >> 12)));
-            v = gl::mul(v, f);
-        } else if (a.post == POST_CANON) {
-            v = gl::canon(v);
-        }
-        D[pos] = v;
-    }
+    store_tile<K, LGL, DIF>(sm, a, D, base, lob, s0, tw_shift);
 }
 
 template <int K, int LGL, bool DIF>
