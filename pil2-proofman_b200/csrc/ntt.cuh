@@ -374,7 +374,7 @@ __device__ __forceinline__ void phases_fixed(uint64_t *sm)
     }
 }
 
-constexpr int log2_const(int x) { return x <= 1 ? 0 : 1 + log2_const(x >> 1); }
+__host__ __device__ constexpr int log2_const(int x) { return x <= 1 ? 0 : 1 + log2_const(x >> 1); }
 
 // Thread / iteration decomposition of a fixed-shape tile.  Element q = threadIdx.x + it * NT of the
 // tile is (mid, lane) = (q >> LGL, q & Lm).  When NT is a multiple of 2^LGL (SPLIT) a thread keeps
@@ -391,7 +391,10 @@ struct Iter {
     static constexpr bool SPLIT = (T % NT == 0) && LOG_NT >= LGL && (1 << (K + LGL)) == T;
     static constexpr int MB = SPLIT ? LOG_NT - LGL : 0;
     static constexpr int LOG_IT = SPLIT ? K - MB : 0;
-    static constexpr int CH = IT < 4 ? IT : 4;  // independent product chains (latency)
+    static constexpr int CH = IT < 4 ? IT : 4;  // independent product chains of the load side (latency)
+    // the store side holds its chains while the tile is read back: two keep the inverse windows
+    // inside the 64-register budget
+    static constexpr int CH_STORE = IT < 2 ? IT : 2;
 };
 
 // Running powers f(it') = A * B^it' for it' = 0 .. IT-1, as CH interleaved chains: chain c yields
@@ -419,8 +422,8 @@ struct Powers {
 };
 
 // The inter-window twiddles of this thread's elements, w_{2^(s0+K)}^(brev_K(mid) * lo) (SPLIT shapes).
-template <int K, int LGL>
-__device__ __forceinline__ void window_twiddles(Powers<Iter<K, LGL>::CH> &pw, uint32_t lob, uint32_t tw_shift, bool inv)
+template <int K, int LGL, int CH>
+__device__ __forceinline__ void window_twiddles(Powers<CH> &pw, uint32_t lob, uint32_t tw_shift, bool inv)
 {
     using I = Iter<K, LGL>;
     constexpr uint32_t Lm = (1u << LGL) - 1;
@@ -428,6 +431,39 @@ __device__ __forceinline__ void window_twiddles(Powers<Iter<K, LGL>::CH> &pw, ui
     const uint32_t M0 = threadIdx.x >> LGL;
     const uint32_t e0 = (brev_bits(M0, I::MB) << I::LOG_IT) * lo;  // < 2^(s0 + K) <= 2^26
     pw.init(big_twiddle((uint64_t)e0 << tw_shift, inv), big_twiddle((uint64_t)lo << tw_shift, inv));
+}
+
+// First forward window of an LDE at blowup 2^LGL (s0 = rep = LGL): the tile's 2^LGL lanes of a mid
+// are copies of one source element (the zero padding folded away), lane l twiddled by t^l with
+// t = w_{2^(s0+K)}^brev_K(mid).  Each thread loads its sources once (mid = threadIdx.x + i * NT,
+// coalesced), forms t as a running product over i in bit-reversed order, and writes all lanes.
+template <int K, int LGL>
+__device__ __forceinline__ void load_tile_copies(uint64_t *sm, const uint64_t *S, uint32_t base, uint32_t tw_shift)
+{
+    constexpr int NT = Shape<K, LGL>::NT, LOG_NT = log2_const(NT);
+    constexpr int NI = (1 << K) / NT, LOG_NI = K - LOG_NT;  // sources per thread
+    constexpr int CH = NI < 4 ? NI : 4;
+    static_assert((1 << K) % NT == 0 && K >= LOG_NT, "copy-lane load needs NT | 2^K");
+    const uint64_t *src = S + (base >> LGL);
+    Powers<CH> pw;
+    pw.init(big_twiddle((uint64_t)(brev_bits(threadIdx.x, LOG_NT) << LOG_NI) << tw_shift, false),
+            big_twiddle((uint64_t)1 << tw_shift, false));
+#pragma unroll 1
+    for (int jj = 0; jj < NI; jj += CH) {
+#pragma unroll
+        for (int c = 0; c < CH; c++) {
+            const uint32_t mid = threadIdx.x + brev_bits((uint32_t)(jj + c), LOG_NI) * NT;
+            const uint64_t v = src[mid];
+            const uint64_t t = pw.next(c);
+            uint64_t u = v;
+            sm[pad16(mid << LGL)] = v;
+#pragma unroll
+            for (int l = 1; l < (1 << LGL); l++) {
+                u = gl::mul(u, t);
+                sm[pad16((mid << LGL) | l)] = u;
+            }
+        }
+    }
 }
 
 // Register-path tile load of a fixed-shape window: the gather (with the Q stage's source remap
@@ -442,9 +478,15 @@ __device__ __forceinline__ void load_tile(uint64_t *sm, const Pass &a, const uin
     constexpr uint32_t Lm = (1u << LGL) - 1;
     const uint32_t rep = a.rep, gshift = a.gshift, goff = (uint32_t)a.goff;
     const bool tw = !DIF && s0 > 0;
+    if constexpr (!DIF && LGL >= 1 && LGL <= 2 && K >= log2_const(Shape<K, LGL>::NT)) {
+        if (rep == LGL && s0 == LGL && gshift == 0 && goff == 0 && a.scale == 0) {
+            load_tile_copies<K, LGL>(sm, S, base, tw_shift);
+            return;
+        }
+    }
     if constexpr (I::SPLIT) {
         Powers<I::CH> pw;
-        if (tw) window_twiddles<K, LGL>(pw, lob, tw_shift, false);
+        if (tw) window_twiddles<K, LGL, I::CH>(pw, lob, tw_shift, false);
 #pragma unroll 1
         for (int jj = 0; jj < IT; jj += I::CH) {
 #pragma unroll
@@ -489,9 +531,9 @@ __device__ __forceinline__ void store_tile(const uint64_t *sm, const Pass &a, ui
     const bool tw = DIF && s0 > 0;
     const uint32_t post = a.post;
     if constexpr (I::SPLIT) {
-        Powers<I::CH> pw;
+        Powers<I::CH_STORE> pw;
         if (tw) {
-            window_twiddles<K, LGL>(pw, lob, tw_shift, true);
+            window_twiddles<K, LGL, I::CH_STORE>(pw, lob, tw_shift, true);
         } else if (post == POST_COSET) {
             // pos = base | q (s0 = 0, LGL = 0), base = hi << K: brev_lg(pos) = brev_lg(base) +
             // ((brev_MB(tid) << LOG_IT) + brev_LOG_IT(it)) << (lg - K)
@@ -504,9 +546,9 @@ __device__ __forceinline__ void store_tile(const uint64_t *sm, const Pass &a, ui
             pw.init(c0, st);
         }
 #pragma unroll 1
-        for (int jj = 0; jj < IT; jj += I::CH) {
+        for (int jj = 0; jj < IT; jj += I::CH_STORE) {
 #pragma unroll
-            for (int c = 0; c < I::CH; c++) {
+            for (int c = 0; c < I::CH_STORE; c++) {
                 const uint32_t it = brev_bits((uint32_t)(jj + c), I::LOG_IT);
                 const uint32_t q = threadIdx.x + it * NT;
                 const uint32_t pos = base | ((q >> LGL) << s0) | (q & Lm);
