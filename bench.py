@@ -177,14 +177,15 @@ def host_ram_gb():
 TRACE_SEED = 1000  # seed of the benchmarked trace on every rank (tests/golden/full_size.json pins its root)
 
 
-def full_size_fixture(wl):
-    """The reference CPU build's root for this workload's seeded trace, if make_full_size.py recorded it."""
+def full_size_fixture(wl, family):
+    """The reference CPU build's root for this workload's seeded trace under this hash family, if
+    make_full_size.py recorded it."""
     path = os.path.join(REPO, "tests", "golden", "full_size.json")
     try:
         with open(path) as f:
             for s in json.load(f)["shapes"]:
-                if (s["nBits"], s["nBitsExt"], s["nCols"], s["arity"], s["seed"]) == (
-                        wl["nbits"], wl["nbits_ext"], wl["ncols"], wl["arity"], TRACE_SEED):
+                if (s["nBits"], s["nBitsExt"], s["nCols"], s["arity"], s["seed"], s.get("family", 2)) == (
+                        wl["nbits"], wl["nbits_ext"], wl["ncols"], wl["arity"], TRACE_SEED, family):
                     return s
     except (OSError, KeyError, ValueError):
         pass
@@ -246,7 +247,7 @@ def run_reference(args, wl):
     if rank != 0:
         return 0
     val, sec, threads, sample, root = time_reference_cpu(wl, args.steps, args.warmup, args.hash_family)
-    fx = full_size_fixture(wl) if args.hash_family == 2 else None
+    fx = full_size_fixture(wl, args.hash_family)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(val, 6), "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3),
@@ -425,7 +426,7 @@ def finish(args, wl, pkg, dist, rank, world, value, ms, launches, kernel_ms, roo
     nbits, nbe, ncols, arity = wl["nbits"], wl["nbits_ext"], wl["ncols"], wl["arity"]
     N = 1 << nbits
     w = 4 * arity
-    fx = full_size_fixture(wl) if args.hash_family == 2 else None
+    fx = full_size_fixture(wl, args.hash_family)
     if fx is not None and [int(v) for v in roots[0]] != fx["root"]:
         raise RuntimeError("root %s differs from the reference CPU root %s of the same trace (full_size.json)"
                            % ([hex(int(v)) for v in roots[0]], [hex(v) for v in fx["root"]]))

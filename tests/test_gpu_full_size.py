@@ -9,12 +9,15 @@ at blowup 4), where the NTT runs its largest windows and the tree its deepest le
 * At the full C2 (2^22 x 256, blowup 2) and C4 (2^20 x 780, blowup 4) shapes, every column:
   the one-pass device commit and the reference-facing commit_witness path against the reference's
   own CPU build run on the same seeded trace (tests/golden/full_size.json, written by
-  make_full_size.py): root, the SHA-256 of the whole tree buffer, and sampled LDE rows.
+  make_full_size.py): root, the SHA-256 of the whole tree buffer, and sampled LDE rows.  The C2
+  trace is also committed with Poseidon1 (hash family 1, PoseidonGoldilocks<16>::merkletree).
 Calls go through the C-ABI library; torch only allocates device memory.
 """
 import hashlib
 import json
 import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -24,6 +27,7 @@ import oracle
 pytestmark = pytest.mark.gpu
 
 P = np.uint64(oracle.P)
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 @pytest.fixture(scope="module")
@@ -92,14 +96,15 @@ def _sha(a):
 @pytest.mark.parametrize("fx", _full_size_fixtures(), ids=lambda fx: fx["name"])
 def test_full_size_matches_reference_cpu(dev, fx):
     """The full workload shapes, every column, against the reference CPU build's commit of the same
-    seeded trace (NTT_Goldilocks::LDE + Poseidon2Goldilocks<16>::merkletree, run by
+    seeded trace (NTT_Goldilocks::LDE + Poseidon2Goldilocks<16>::merkletree, or
+    PoseidonGoldilocks<16>::merkletree for the family-1 record, run by
     make_full_size.py): the one-pass device commit (root, the whole tree buffer by SHA-256, sampled
     LDE rows word for word), then commit_witness from pinned host memory (column blocks of 16, 24,
     48, then 64, crossing PCIe while earlier blocks are extended; the sponge absorbed in 12-column
     chunks on the idle device) to the same root."""
-    import ctypes
     pkg, torch = dev
     nbits, nbe, ncols, arity = fx["nBits"], fx["nBitsExt"], fx["nCols"], fx["arity"]
+    family = fx.get("family", 2)
     N, NExt = 1 << nbits, 1 << nbe
     want_root = np.array(fx["root"], dtype=np.uint64)
     d_trace = torch.empty(N * ncols, dtype=torch.int64, device="cuda")
@@ -107,8 +112,12 @@ def test_full_size_matches_reference_cpu(dev, fx):
     d_lde = torch.empty(NExt * ncols, dtype=torch.int64, device="cuda")
     d_tree = torch.empty(pkg.tree_num_elements(NExt, arity), dtype=torch.int64, device="cuda")
     d_scr = torch.empty(pkg.lde_scratch_words(nbits, ncols), dtype=torch.int64, device="cuda")
-    root_dev = pkg.commit_device(d_lde, d_tree, d_trace, nbits, nbe, ncols, arity, d_scr)
-    torch.cuda.synchronize()
+    pkg.set_native_hash_family(family)
+    try:
+        root_dev = pkg.commit_device(d_lde, d_tree, d_trace, nbits, nbe, ncols, arity, d_scr)
+        torch.cuda.synchronize()
+    finally:
+        pkg.set_native_hash_family(2)
     assert (root_dev == want_root).all(), ([hex(int(v)) for v in root_dev], [hex(v) for v in fx["root"]])
     tree = d_tree.cpu().numpy().view(np.uint64)
     assert tree.size == fx["tree_words"]
@@ -119,21 +128,57 @@ def test_full_size_matches_reference_cpu(dev, fx):
     block = d_rows_out.cpu().numpy().view(np.uint64).reshape(-1, ncols)
     assert [int(v) for v in block[0]] == fx["sample_row0"]
     assert _sha(block) == fx["sample_rows_sha256"]
-    host = torch.empty(N * ncols, dtype=torch.int64, pin_memory=True)
-    host.copy_(d_trace)
-    del d_trace, d_lde, d_tree, d_scr, d_rows_out
-    torch.cuda.empty_cache()
+    del d_lde, d_tree, d_scr, d_rows_out
+    if family != 2:
+        # the reference entry points take set_hash_family once per process: Poseidon1 runs in a child
+        del d_trace
+        torch.cuda.empty_cache()
+        r = subprocess.run([sys.executable, "-c", _WITNESS_CHILD, REPO, str(nbits), str(nbe), str(ncols), str(arity),
+                            str(fx["seed"]), str(family)], capture_output=True, text=True, timeout=900)
+        assert r.returncode == 0, r.stderr[-2000:]
+        root = np.array(json.loads(r.stdout.strip().splitlines()[-1])["root"], dtype=np.uint64)
+    else:
+        host = torch.empty(N * ncols, dtype=torch.int64, pin_memory=True)
+        host.copy_(d_trace)
+        del d_trace
+        torch.cuda.empty_cache()
+        pkg.set_hash_family(2)
+        root = _commit_witness(pkg, host.data_ptr(), nbits, nbe, ncols, arity)
+    assert (root == want_root).all(), (root, want_root)
+
+
+def _commit_witness(pkg, host_ptr, nbits, nbe, ncols, arity):
+    """commit_witness through a StarkShape setup from a pinned host trace, on two streams"""
+    import ctypes
     lib = pkg.load()
-    pkg.set_hash_family(2)
     bufs = pkg.DeviceBuffers(arity=arity, n_streams=2)
     try:
         shape = pkg.StarkShape(nbits, nbe, ncols, arity)
         params = pkg.StepsParams()
-        params.trace = host.data_ptr()
+        params.trace = host_ptr
         root = np.zeros(4, dtype=np.uint64)
         assert lib.commit_witness(shape.setup_ptr, ctypes.addressof(params), 0, 0, 0, root.ctypes.data, bufs.ptr, b"") < 2
         lib.get_stream_proofs(bufs.ptr)
         assert bufs.error() == 0, lib.b200_last_error()
     finally:
         bufs.close()
-    assert (root == want_root).all(), (root, want_root)
+    return root
+
+
+_WITNESS_CHILD = r"""
+import json, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+sys.path.insert(0, sys.argv[1] + "/tests")
+import torch
+from conftest import load_package
+from test_gpu_full_size import _commit_witness
+nbits, nbe, ncols, arity, seed, family = map(int, sys.argv[2:8])
+pkg = load_package()
+pkg.init(0)
+pkg.set_hash_family(family)
+host = torch.empty((1 << nbits) * ncols, dtype=torch.int64, pin_memory=True)
+pkg.load().b200_fill_random_host(host.data_ptr(), host.numel(), seed)
+root = _commit_witness(pkg, host.data_ptr(), nbits, nbe, ncols, arity)
+print(json.dumps({"root": [int(v) for v in root]}))
+"""
