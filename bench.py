@@ -677,10 +677,14 @@ def serve_stream(lib, pool, hosts, arrivals, picks, mode, budget_gb, slots, time
     return lat, wall, roots, stats
 
 
-def serve_rates(rates, duration, n_c3, budget_gb, slots, timeout_s, serial=True):
+def serve_rates(rates, duration, n_c3, budget_gb, slots, timeout_s, serial=True, repeats=1):
     """Poisson request streams at each rate for `duration` seconds of arrivals, served by the
     continuous-batching server and by the FIFO server on the same arrivals; p50/p99 latency and
-    GElem/s of each, and the GElem/s of serial plain commits of the same request list."""
+    GElem/s of each, and the GElem/s of serial plain commits of the same request list.  With
+    repeats > 1 each mode serves the stream that many times, the modes alternating in mirrored order
+    (batching, FIFO, FIFO, batching, ...) so that neither always runs first; the latencies reported
+    are the means over a mode's runs, each run kept under "runs".  Near saturation a few percent of
+    throughput moves the queueing delay a lot, so single runs of the two modes compare poorly."""
     pkg = load_package()
     pkg.init(0)
     lib = pkg.load()
@@ -694,14 +698,24 @@ def serve_rates(rates, duration, n_c3, budget_gb, slots, timeout_s, serial=True)
         elems = sum((1 << pool[p][1]) * pool[p][2] for p in picks)
         entry = {"rate_per_s": rate, "requests": nreq, "arrivals_s": round(float(arrivals[-1]), 2)}
         all_roots = []
-        for mode, name in ((1, "continuous_batching"), (0, "fifo")):
-            lat, wall, roots, stats = serve_stream(lib, pool, hosts, arrivals, picks, mode, budget_gb, slots,
-                                                   timeout_s)
-            all_roots.append(roots)
-            entry[name] = {"wall_s": round(wall, 3), "throughput_gelem_s": round(elems / wall / 1e9, 4),
-                           "p50_ms": round(float(np.percentile(lat, 50)), 2),
-                           "p99_ms": round(float(np.percentile(lat, 99)), 2),
-                           "max_ms": round(float(np.max(lat)), 2), **stats}
+        modes = ((1, "continuous_batching"), (0, "fifo"))
+        runs = {name: [] for _, name in modes}
+        for k in range(repeats):
+            for mode, name in (modes if k % 2 == 0 else modes[::-1]):
+                lat, wall, roots, stats = serve_stream(lib, pool, hosts, arrivals, picks, mode, budget_gb, slots,
+                                                       timeout_s)
+                all_roots.append(roots)
+                runs[name].append({"wall_s": round(wall, 3), "throughput_gelem_s": round(elems / wall / 1e9, 4),
+                                   "p50_ms": round(float(np.percentile(lat, 50)), 2),
+                                   "p99_ms": round(float(np.percentile(lat, 99)), 2),
+                                   "max_ms": round(float(np.max(lat)), 2), **stats})
+        for name, rs in runs.items():
+            if len(rs) == 1:
+                entry[name] = rs[0]
+            else:
+                entry[name] = {key: round(float(np.mean([r[key] for r in rs])), 4 if key.startswith("through") else 2)
+                               for key in ("wall_s", "throughput_gelem_s", "p50_ms", "p99_ms", "max_ms")}
+                entry[name]["runs"] = rs
         if serial:
             # the same request list as plain commits one after another, all queued at time 0
             _, wall, roots, _ = serve_stream(lib, pool, hosts, np.zeros(nreq), picks, 0, budget_gb, 1, timeout_s)
@@ -724,14 +738,15 @@ def run_serving(args):
     budget; each request's LDE and tree stay resident until it completes and is released."""
     rates = [float(r) for r in args.rates.split(",")]
     per_rate, npool = serve_rates(rates, args.duration, args.pool, args.serve_budget_gb, args.slots,
-                                  args.serve_timeout)
+                                  args.serve_timeout, repeats=args.serve_repeats)
     line = {"metric": "served commit stream: request latency p50/p99 and throughput, continuous batching vs FIFO",
             "workload": "c5", "unit": "ms", "value": per_rate[0]["continuous_batching"]["p99_ms"],
             "higher_is_better": False, "per_rate": per_rate,
             "config": {"workload": "Poisson arrivals for %.0f s per rate; shapes: %d drawn from the 64-instance C3 "
                                    "distribution (80%%) and 2^20 x 780 blowup 4 (20%%); Poseidon2 W16 arity 4"
                                    % (args.duration, npool - 1),
-                       "device_budget_gib": args.serve_budget_gb, "slots": args.slots},
+                       "device_budget_gib": args.serve_budget_gb, "slots": args.slots,
+                       "runs_per_mode": args.serve_repeats},
             "n_gpus": 1, "dtype": "u64", "data": "synthetic (seeded uniform Goldilocks)"}
     print(json.dumps(line), flush=True)
     return 0
@@ -895,6 +910,8 @@ def main():
     ap.add_argument("--slots", type=int, default=4, help="c5: server slots (units admitted at once)")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0, help="c5: server device-memory budget")
     ap.add_argument("--serve-timeout", type=float, default=1800.0, help="c5: give up after this many seconds")
+    ap.add_argument("--serve-repeats", type=int, default=2,
+                    help="c5: runs of each mode on the same stream, in mirrored order (batching, FIFO, FIFO, ...)")
     ap.add_argument("--no-legs", action="store_true",
                     help="default workload: skip the batched (c3) and served (c5) legs of the JSON line")
     ap.add_argument("--serve-seconds", type=float, default=30.0,
