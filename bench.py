@@ -624,6 +624,26 @@ def serve_pool(lib, n_c3, seed=12):
     return pool, hosts
 
 
+def gpu_timeline(units):
+    """Device timeline of a served stream from its units' (copies issued, copies done, kernels
+    started, kernels done) times: ms with kernels running; the gaps between one unit's kernels and
+    the next, split into the part before the next unit was issued (no request waiting, or the host
+    admitted it late) and the part after (its host-to-device copy had not landed: the GPU waited
+    for PCIe)."""
+    spans = sorted((st, dn, iss) for iss, cp, st, dn in units if st >= 0 and dn >= 0)
+    if not spans:
+        return {}
+    busy = sum(dn - st for st, dn, _ in spans)
+    copy_wait = not_issued = 0.0
+    for (_, prev_dn, _), (st, _, iss) in zip(spans, spans[1:]):
+        gap = max(0.0, st - prev_dn)
+        late = min(gap, max(0.0, iss - prev_dn))
+        not_issued += late
+        copy_wait += gap - late
+    return {"gpu_kernels_ms": round(busy, 1), "gpu_waiting_for_copy_ms": round(copy_wait, 1),
+            "gpu_idle_before_issue_ms": round(not_issued, 1), "gpu_span_ms": round(spans[-1][1] - spans[0][0], 1)}
+
+
 def serve_stream(lib, pool, hosts, arrivals, picks, mode, budget_gb, slots, timeout_s):
     """Submit requests at the given arrival times to a commit server (mode 1 continuous batching,
     0 FIFO); returns (latencies ms, wall s, roots, stats)."""
@@ -661,17 +681,20 @@ def serve_stream(lib, pool, hosts, arrivals, picks, mode, budget_gb, slots, time
                 raise RuntimeError("served stream did not finish within %.0f s" % timeout_s)
             time.sleep(0.001)
         wall = time.perf_counter() - t0
-        st = (ctypes.c_uint64 * 5)()
-        lib.b200_server_stats(srv, st, 5)
-        times = (ctypes.c_double * 3)()
-        waits, service = [], []
+        st = (ctypes.c_uint64 * 6)()
+        lib.b200_server_stats(srv, st, 6)
+        times, g = (ctypes.c_double * 3)(), (ctypes.c_double * 4)()
+        waits, service, units = [], [], set()
         for rid in ids:
             lib.b200_server_request_times(srv, rid, times)
             waits.append(times[1] - times[0])
             service.append(times[2] - times[1])
+            lib.b200_server_request_gpu_times(srv, rid, g)
+            units.add(tuple(g))  # a batched unit's requests share its timeline
         stats = {"plain_units": st[0], "batched_units": st[1], "batched_requests": st[2], "pool_trims": st[3],
-                 "overtakes": st[4], "mean_wait_to_admission_ms": round(float(np.mean(waits)), 2),
-                 "mean_admission_to_done_ms": round(float(np.mean(service)), 2)}
+                 "overtakes": st[4], "host_enqueue_ms": round(st[5] / 1e3, 1),
+                 "mean_wait_to_admission_ms": round(float(np.mean(waits)), 2),
+                 "mean_admission_to_done_ms": round(float(np.mean(service)), 2), **gpu_timeline(units)}
     finally:
         lib.b200_server_free(srv)
     return lat, wall, roots, stats
@@ -689,6 +712,9 @@ def serve_rates(rates, duration, n_c3, budget_gb, slots, timeout_s, serial=True,
     pkg.init(0)
     lib = pkg.load()
     pool, hosts = serve_pool(lib, n_c3)
+    # untimed warm-up: every shape once through each mode (module loading, first device allocations)
+    for mode in (1, 0):
+        serve_stream(lib, pool, hosts, np.zeros(len(pool)), list(range(len(pool))), mode, budget_gb, slots, timeout_s)
     rng = np.random.Generator(np.random.PCG64(11))
     out = []
     for rate in rates:

@@ -288,11 +288,16 @@ void *b200_server_new(int device, uint64_t budget_bytes, uint32_t slots);
  * batched unit, default 64). */
 int b200_server_configure(void *srv, int batching, uint64_t small_elems, uint32_t max_batch);
 /* counters into out[0..n): plain units, batched units, requests in batched units, pool trims (an
- * admission that did not fit the pool's cached blocks), times a waiting request was passed */
+ * admission that did not fit the pool's cached blocks), times a waiting request was passed,
+ * microseconds the worker spent enqueueing units (allocations, copies, launches) */
 int b200_server_stats(void *srv, uint64_t *out, uint64_t n);
 /* submission, admission and completion time of a request in ms since the server was created
  * (times3[1], times3[2] = -1 until reached) */
 int b200_server_request_times(void *srv, int64_t id, double *times3);
+/* device timeline of a completed request's unit in ms of device time since the server was created:
+ * copies issued (the unit reached its stream), host-to-device copies done, kernels started (copies
+ * done and the unit ahead finished), kernels done; -1 until the request completes */
+int b200_server_request_gpu_times(void *srv, int64_t id, double *times4);
 /* returns a request id > 0, or B200_EBUSY if the request can never fit the budget */
 int64_t b200_server_submit(void *srv, const uint64_t *host_trace, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols,
                            uint64_t arity, uint64_t *root_out);

@@ -100,6 +100,7 @@ _SIGS = {
     "b200_server_configure": (_i32, [_vp, _i32, _u64, ctypes.c_uint32]),
     "b200_server_stats": (_i32, [_vp, _pu64, _u64]),
     "b200_server_request_times": (_i32, [_vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)]),
+    "b200_server_request_gpu_times": (_i32, [_vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)]),
     # query openings, Q stage, plan autotuner, packed witness
     "b200_query_proof_words": (_u64, [_u64, _u64, _u64, _u64]),
     "b200_query_openings_device": (_i32, [_vp, _vp, _u64, _u64, _vp, _u64, _u64, _vp, _u64, _vp]),

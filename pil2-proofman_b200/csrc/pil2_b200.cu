@@ -649,11 +649,100 @@ static void commit_blocks(uint64_t nBits, uint64_t nCols, std::vector<uint64_t> 
     if (nCols) starts.push_back(nCols);
 }
 
+// Device buffers of one pipelined commit (pipelined_commit).  `staging` (N * nCols words) receives
+// the row-major column blocks, block [c0, c0 + cb) at staging + c0 * N with row pitch cb; `cm1`
+// (N * nCols) receives the column-major trace and `scratch` (N * nCols) is the LDE's work area,
+// which may be cm1 itself (the LDE then runs in place on the transposed trace).
+struct PipeBuffers {
+    uint64_t *staging = nullptr, *cm1 = nullptr, *scratch = nullptr, *lde = nullptr, *tree = nullptr;
+    uint64_t *h_root = nullptr;  // pinned 4 words for the root (null: left in the tree)
+};
+
+// H2D + LDE + tree (+ root D2H) of a row-major host trace, pipelined over column blocks: the blocks
+// cross PCIe on `copy`, each a 2-D copy into its staging block; `comp` transposes each block into
+// cm1 as soon as it has landed and extends it into the LDE, so the LDE of a block overlaps the copy
+// of the next, then hashes the rows once every column is extended.  `copy` first waits for
+// `copy_after` and `comp` for `comp_after` (either may be null).  block_ev needs one event per
+// column block (commit_blocks); h2d_done (nullable) is recorded after the last copy and
+// comp_started (nullable) on `comp` once the first block has landed and comp_after has passed.
+//
+// With `idle` (nothing else runs on the device, so the copy is exposed), an arity-4 commit hashes
+// its rows while the later column blocks are still crossing: the row sponge in 12-column chunks
+// (stream::absorb_kernel, the 4-word state carried in tree level 0), each chunk as soon as its
+// columns are extended.  Same sponge, same digests.
+static int pipelined_commit(const uint64_t *trace, uint64_t nBits, uint64_t nBitsExt, uint64_t nCols, uint64_t arity,
+                            int fam, const PipeBuffers &pb, cudaStream_t copy, cudaStream_t comp,
+                            std::vector<cudaEvent_t> &block_ev, cudaEvent_t h2d_done, cudaEvent_t copy_after,
+                            cudaEvent_t comp_after, bool idle, cudaEvent_t comp_started = nullptr)
+{
+    const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
+    const uint64_t tsz = merkle::tree_num_elements(NExt, arity);
+    std::vector<uint64_t> starts;
+    commit_blocks(nBits, nCols, starts);
+    const uint64_t nblk = starts.size() - 1;
+    while (block_ev.size() < nblk) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        block_ev.push_back(e);
+    }
+    if (copy_after) CK(cudaStreamWaitEvent(copy, copy_after, 0), "copy order");
+    for (uint64_t k = 0; k < nblk; k++) {
+        const uint64_t c0 = starts[k], cb = starts[k + 1] - c0;
+        if (cb == nCols)
+            CK(cudaMemcpyAsync(pb.staging, trace, N * nCols * 8, cudaMemcpyHostToDevice, copy), "trace H2D");
+        else
+            CK(cudaMemcpy2DAsync(pb.staging + c0 * N, cb * 8, trace + c0, nCols * 8, cb * 8, N, cudaMemcpyHostToDevice,
+                                 copy),
+               "trace block H2D");
+        CK(cudaEventRecord(block_ev[k], copy), "event");
+    }
+    if (h2d_done) CK(cudaEventRecord(h2d_done, copy), "event");
+    const bool chunked = idle && arity == 4 && nblk > 1;
+    uint64_t next_chunk = 0;
+    if (comp_after) CK(cudaStreamWaitEvent(comp, comp_after, 0), "order commits");
+    for (uint64_t k = 0; k < nblk; k++) {
+        const uint64_t c0 = starts[k], cb = starts[k + 1] - c0;
+        CK(cudaStreamWaitEvent(comp, block_ev[k], 0), "block landed");
+        if (k == 0 && comp_started) CK(cudaEventRecord(comp_started, comp), "event");
+        {
+            prof::Scope ps(prof::TRANSPOSE, comp);
+            CK(ntt::transpose(pb.cm1 + c0 * N, pb.staging + c0 * N, N, cb, N, comp), "transpose");
+        }
+        CK(ntt::lde(pb.lde + c0 * NExt, pb.cm1 + c0 * N, false, (uint32_t)nBits, (uint32_t)nBitsExt, cb,
+                    pb.scratch + c0 * N, comp),
+           "lde");
+        if (chunked) {
+            const uint64_t avail = k + 1 == nblk ? nCols : c0 + cb;  // columns extended so far
+            prof::Scope ps(prof::LEAF_HASH, comp);
+            for (; next_chunk * stream::RATE < nCols; next_chunk++) {
+                const uint64_t a0 = next_chunk * stream::RATE;
+                const uint32_t cc = (uint32_t)std::min<uint64_t>(stream::RATE, nCols - a0);
+                if (a0 + cc > avail) break;
+                const unsigned grid = (unsigned)((NExt + merkle::TPB - 1) / merkle::TPB);
+                if (fam == 1)
+                    stream::absorb_kernel<1><<<grid, merkle::TPB, 0, comp>>>(pb.tree, pb.lde + a0 * NExt, cc,
+                                                                             next_chunk == 0, NExt);
+                else
+                    stream::absorb_kernel<2><<<grid, merkle::TPB, 0, comp>>>(pb.tree, pb.lde + a0 * NExt, cc,
+                                                                             next_chunk == 0, NExt);
+                prof::count();
+                CK(cudaGetLastError(), "absorb");
+            }
+        }
+    }
+    if (chunked) {
+        const cudaError_t e = fam == 1 ? merkle::build_levels<16, 1>(pb.tree, NExt, comp)
+                                       : merkle::build_levels<16, 2>(pb.tree, NExt, comp);
+        CK(e, "tree levels");
+    } else
+        CK(merkle::build_tree_arity(arity, pb.tree, pb.lde, 1, NExt, nCols, NExt, comp, fam), "merkletree");
+    if (pb.h_root)
+        CK(cudaMemcpyAsync(pb.h_root, pb.tree + tsz - 4, 32, cudaMemcpyDeviceToHost, comp), "root D2H");
+    return B200_OK;
+}
+
 // Enqueue H2D + LDE + tree + root D2H for a row-major host trace on a slot, into the regions of the
-// slot's prover buffer that `lay` names.  The trace crosses PCIe in column blocks on the slot's copy
-// stream, each a 2-D copy into a row-major N x B staging block; the compute stream transposes each
-// block into ("cm1", false) as soon as it has landed and extends it into ("cm1", true), so the LDE of
-// a block overlaps the copy of the next, then hashes the rows once every column is extended.
+// slot's prover buffer that `lay` names (pipelined_commit over the slot's copy and compute streams).
 //
 // The staging area is the top N * nCols words of the ("cm1", true) region, as the reference stages
 // its trace in that region (commit_witness_gpu, starks_api.cu:1651-1659).  The LDE of the blocks up
@@ -664,86 +753,32 @@ static void commit_blocks(uint64_t nBits, uint64_t nCols, std::vector<uint64_t> 
 // reference's preserve_src LDE leaves it.
 //
 // The compute stream also waits for the previously issued commit to end (see
-// CommitBuffers::last_end); the copy stream only for this slot's previous commit.
+// CommitBuffers::last_end); the copy stream only for this slot's previous commit (which may still
+// read the staging area).  With an earlier commit still running, this commit's copy hides under it
+// and its kernels wait for it anyway; with the device idle the copy is exposed and the rows are
+// hashed in chunks while the later blocks cross.
 static int slot_commit(CommitBuffers *b, Slot &s, const uint64_t *trace, uint64_t nBits, uint64_t nBitsExt,
                        uint64_t nCols, uint64_t arity, const CommitLayout &lay)
 {
     const uint64_t N = 1ull << nBits, NExt = 1ull << nBitsExt;
-    const uint64_t tsz = merkle::tree_num_elements(NExt, arity);
     int rc;
     if ((rc = grow(s.d_aux, s.cap_aux, lay.words)) || (rc = grow(s.d_scratch, s.cap_scratch, N * nCols))) return rc;
     s.d_lde = s.d_aux + lay.cm1_ext;
     s.d_tree = s.d_aux + lay.mt1;
     s.d_cm1 = s.d_aux + lay.cm1;
     s.aux_words = lay.words;
-    uint64_t *staging = s.d_lde + (NExt - N) * nCols;
-    std::vector<uint64_t> starts;
-    commit_blocks(nBits, nCols, starts);
-    const uint64_t nblk = starts.size() - 1;
-    while (s.blocks.size() < nblk) {
-        cudaEvent_t e;
-        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-        s.blocks.push_back(e);
-    }
-    // the copy may overwrite the staging area once this slot's previous commit is done with it
-    CK(cudaStreamWaitEvent(s.copy, s.end, 0), "slot reuse");
-    for (uint64_t k = 0; k < nblk; k++) {
-        const uint64_t c0 = starts[k], cb = starts[k + 1] - c0;
-        if (cb == nCols)
-            CK(cudaMemcpyAsync(staging, trace, N * nCols * 8, cudaMemcpyHostToDevice, s.copy), "trace H2D");
-        else
-            CK(cudaMemcpy2DAsync(staging + c0 * N, cb * 8, trace + c0, nCols * 8, cb * 8, N, cudaMemcpyHostToDevice,
-                                 s.copy),
-               "trace block H2D");
-        CK(cudaEventRecord(s.blocks[k], s.copy), "event");
-    }
-    CK(cudaEventRecord(s.h2d_done, s.copy), "event");
-    // With an earlier commit still running, this commit's copy hides under it and its kernels
-    // wait for it anyway.  With the device idle the copy is exposed, so an arity-4 commit hashes
-    // its rows while the later column blocks are still crossing: the row sponge in 12-column
-    // chunks (stream::absorb_kernel, the 4-word state carried in tree level 0), each chunk as
-    // soon as its columns are extended.  Same sponge, same digests.
-    const int fam = g_hash_family.load();
+    PipeBuffers pb;
+    pb.staging = s.d_lde + (NExt - N) * nCols;
+    pb.cm1 = s.d_cm1;
+    pb.scratch = s.d_scratch;
+    pb.lde = s.d_lde;
+    pb.tree = s.d_tree;
+    pb.h_root = s.h_root;
     const bool idle = !b->last_end || cudaEventQuery(b->last_end) == cudaSuccess;
-    const bool chunked = idle && arity == 4 && nblk > 1;
-    uint64_t next_chunk = 0;
-    if (b->last_end && b->last_end != s.end) CK(cudaStreamWaitEvent(s.stream, b->last_end, 0), "order commits");
-    for (uint64_t k = 0; k < nblk; k++) {
-        const uint64_t c0 = starts[k], cb = starts[k + 1] - c0;
-        CK(cudaStreamWaitEvent(s.stream, s.blocks[k], 0), "block landed");
-        {
-            prof::Scope ps(prof::TRANSPOSE, s.stream);
-            CK(ntt::transpose(s.d_cm1 + c0 * N, staging + c0 * N, N, cb, N, s.stream), "transpose");
-        }
-        CK(ntt::lde(s.d_lde + c0 * NExt, s.d_cm1 + c0 * N, false, (uint32_t)nBits, (uint32_t)nBitsExt, cb,
-                    s.d_scratch + c0 * N, s.stream),
-           "lde");
-        if (chunked) {
-            const uint64_t avail = k + 1 == nblk ? nCols : c0 + cb;  // columns extended so far
-            prof::Scope ps(prof::LEAF_HASH, s.stream);
-            for (; next_chunk * stream::RATE < nCols; next_chunk++) {
-                const uint64_t a0 = next_chunk * stream::RATE;
-                const uint32_t cc = (uint32_t)std::min<uint64_t>(stream::RATE, nCols - a0);
-                if (a0 + cc > avail) break;
-                const unsigned grid = (unsigned)((NExt + merkle::TPB - 1) / merkle::TPB);
-                if (fam == 1)
-                    stream::absorb_kernel<1><<<grid, merkle::TPB, 0, s.stream>>>(s.d_tree, s.d_lde + a0 * NExt, cc,
-                                                                                 next_chunk == 0, NExt);
-                else
-                    stream::absorb_kernel<2><<<grid, merkle::TPB, 0, s.stream>>>(s.d_tree, s.d_lde + a0 * NExt, cc,
-                                                                                 next_chunk == 0, NExt);
-                prof::count();
-                CK(cudaGetLastError(), "absorb");
-            }
-        }
-    }
-    if (chunked) {
-        const cudaError_t e = fam == 1 ? merkle::build_levels<16, 1>(s.d_tree, NExt, s.stream)
-                                       : merkle::build_levels<16, 2>(s.d_tree, NExt, s.stream);
-        CK(e, "tree levels");
-    } else
-        CK(merkle::build_tree_arity(arity, s.d_tree, s.d_lde, 1, NExt, nCols, NExt, s.stream, fam), "merkletree");
-    CK(cudaMemcpyAsync(s.h_root, s.d_tree + tsz - 4, 32, cudaMemcpyDeviceToHost, s.stream), "root D2H");
+    cudaEvent_t after = b->last_end && b->last_end != s.end ? b->last_end : nullptr;
+    if ((rc = pipelined_commit(trace, nBits, nBitsExt, nCols, arity, g_hash_family.load(), pb, s.copy, s.stream,
+                               s.blocks, s.h2d_done, s.end, after, idle)))
+        return rc;
     CK(cudaEventRecord(s.end, s.stream), "event");
     b->last_end = s.end;
     return B200_OK;

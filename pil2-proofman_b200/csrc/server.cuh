@@ -8,7 +8,12 @@
 //     and tree levels run as shared grouped launches and a persistent leaf kernel;
 //   * a larger request is a plain unit: the single-instance commit.
 // Units are admitted while earlier ones run: each unit's host-to-device copy overlaps the kernels
-// of the units ahead of it, and each unit's kernels follow the previous unit's on the device.
+// of the units ahead of it, and each unit's kernels follow the previous unit's on the device.  All
+// host-to-device copies go through one copy stream in admission order, so the next unit's trace
+// has the whole PCIe link (copies of different streams would share it and all land late).  A
+// plain unit's trace crosses in column blocks and each block is extended as soon as it lands (the
+// pipeline of commit_witness), so a request that finds the device idle waits for its first
+// block's copy, not its whole trace.
 // Measured on a B200 with the C3 size mix, letting the units' kernels interleave instead (streams
 // of different priorities, no ordering) doubled the median latency at 5 requests/s and lowered the
 // throughput at 20 requests/s by 7 %: every kernel here fills the GPU, and co-resident commits only
@@ -51,6 +56,10 @@ struct Request {
     bool released = false;
     cudaStream_t stream = nullptr;  // the stream its buffers were last used on
     double t_submit = 0, t_admit = 0, t_done = 0;
+    // device timeline of its unit, ms since the server's reference event: copies issued (the unit
+    // reached its stream), host-to-device copies done, kernels started (copies done and the
+    // previous unit finished), kernels done
+    double g_issued = -1, g_copied = -1, g_start = -1, g_done = -1;
     uint32_t overtaken = 0;  // times a batch of smaller requests was admitted ahead of it
     std::string err;  // reason of a failed request (reported to the caller by status())
     uint64_t bytes() const { return 8 * (2 * words_trace + words_lde + words_tree); }
@@ -64,6 +73,7 @@ struct Unit {
     int slot = -1;
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
+    cudaEvent_t issued = nullptr, copied = nullptr, started = nullptr;  // timeline (timing enabled, like done)
     batch::Plan *plan = nullptr;
     unsigned char *d_table = nullptr;  // batched: the plan's device tables (from the pool)
 };
@@ -79,6 +89,8 @@ class Server {
     uint32_t max_batch = 64;               // requests per batched unit
     uint32_t max_overtakes = 4;            // times a waiting request may be overtaken by a batch
     std::vector<cudaStream_t> streams;     // [slot]
+    cudaStream_t copy_stream = nullptr;                // every unit's host-to-device copies, in admission order
+    std::vector<std::vector<cudaEvent_t>> block_events;  // [slot] one per column block of a plain unit
     std::vector<unsigned char *> staging;            // [slot] pinned
     std::vector<uint64_t *> h_roots;                 // [slot] pinned, plain units' root
     std::vector<int> slot_busy;
@@ -91,10 +103,12 @@ class Server {
     bool stop = false, configured = false;
     std::thread worker;
     cudaMemPool_t pool = nullptr;
-    cudaEvent_t last_done = nullptr;  // mode 0: completion of the most recently admitted unit
+    cudaEvent_t last_done = nullptr;  // completion of the most recently admitted unit
+    cudaEvent_t t0_event = nullptr;   // device-time origin of the request timelines
     std::vector<cudaEvent_t> spare_events;
     int family = 2;                   // hash family of this server's commits (fixed at creation)
     uint64_t units_plain = 0, units_batched = 0, batched_requests = 0, pool_trims = 0, overtakes = 0;
+    double launch_ms = 0;  // host time spent enqueueing units (allocations, copies, kernel launches)
     double t_start = 0;
 
     int start(int dev, uint64_t budget_bytes, uint32_t slots)
@@ -118,6 +132,7 @@ class Server {
             cudaStream_t s;
             CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
             streams.push_back(s);
+            block_events.emplace_back();
             unsigned char *st = nullptr;
             uint64_t *hr = nullptr;
             CK(cudaMallocHost((void **)&st, STAGING_BYTES), "pinned staging");
@@ -126,6 +141,9 @@ class Server {
             h_roots.push_back(hr);
             slot_busy.push_back(0);
         }
+        CK(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking), "stream");
+        CK(cudaEventCreate(&t0_event), "event");
+        CK(cudaEventRecord(t0_event, streams[0]), "event record");
         worker = std::thread([this] { loop(); });
         return B200_OK;
     }
@@ -139,6 +157,7 @@ class Server {
         cv.notify_all();
         if (worker.joinable()) worker.join();
         cudaSetDevice(device);
+        if (copy_stream) cudaStreamSynchronize(copy_stream);
         for (cudaStream_t s : streams) cudaStreamSynchronize(s);
         for (Unit *u : running) finish_unit(u, cudaEventQuery(u->done) == cudaSuccess);
         for (auto &kv : all) {
@@ -148,9 +167,13 @@ class Server {
         }
         cudaDeviceSynchronize();
         for (cudaStream_t s : streams) cudaStreamDestroy(s);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+        for (auto &v : block_events)
+            for (cudaEvent_t e : v) cudaEventDestroy(e);
         for (unsigned char *p : staging) cudaFreeHost(p);
         for (uint64_t *p : h_roots) cudaFreeHost(p);
         for (cudaEvent_t e : spare_events) cudaEventDestroy(e);
+        if (t0_event) cudaEventDestroy(t0_event);
         if (pool) cudaMemPoolDestroy(pool);
     }
 
@@ -246,7 +269,7 @@ class Server {
             return e;
         }
         cudaEvent_t e = nullptr;
-        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
         return e;
     }
 
@@ -258,23 +281,38 @@ class Server {
             for (Request *r : u->reqs) r->err = "device buffers for the request could not be allocated";
             return B200_ENOMEM;
         }
-        for (Request *r : u->reqs) {
-            r->stream = s;
-            if (r->words_trace &&
-                cudaMemcpyAsync(r->d_trace, r->trace, 8 * r->words_trace, cudaMemcpyHostToDevice, s) != cudaSuccess)
-                return B200_ECUDA;
-        }
-        // kernels in admission order (the copies above overlap the units ahead)
-        if (last_done && cudaStreamWaitEvent(s, last_done, 0) != cudaSuccess) return B200_ECUDA;
+        if (!(u->issued = take_event()) || cudaEventRecord(u->issued, s) != cudaSuccess) return B200_ECUDA;
+        if (!(u->copied = take_event()) || !(u->started = take_event())) return B200_ECUDA;
         if (!u->batched) {
+            // column blocks on the copy stream once the buffers are allocated (u->issued, on s), the
+            // kernels on s after the unit ahead (last_done)
             Request *r = u->reqs[0];
-            int rc = commit_device_fam(nullptr, r->d_lde, r->d_tree, r->d_trace, 1, r->nBits, r->nBitsExt, r->nCols,
-                                       r->arity, r->d_scratch, s, family);
+            r->stream = s;
+            PipeBuffers pb;
+            pb.staging = r->d_trace;
+            pb.cm1 = pb.scratch = r->d_scratch;
+            pb.lde = r->d_lde;
+            pb.tree = r->d_tree;
+            pb.h_root = h_roots[u->slot];
+            const bool idle = !last_done || cudaEventQuery(last_done) == cudaSuccess;
+            int rc = pipelined_commit(r->trace, r->nBits, r->nBitsExt, r->nCols, r->arity, family, pb,
+                                      copy_stream, s, block_events[u->slot], u->copied, u->issued, last_done,
+                                      idle, u->started);
             if (rc) return rc;
-            if (cudaMemcpyAsync(h_roots[u->slot], r->d_tree + r->words_tree - 4, 32, cudaMemcpyDeviceToHost, s) !=
-                cudaSuccess)
-                return B200_ECUDA;
         } else {
+            // small traces: whole copies on the copy stream (after the allocations), then the batched
+            // kernels on s after the unit ahead
+            if (cudaStreamWaitEvent(copy_stream, u->issued, 0) != cudaSuccess) return B200_ECUDA;
+            for (Request *r : u->reqs) {
+                r->stream = s;
+                if (r->words_trace && cudaMemcpyAsync(r->d_trace, r->trace, 8 * r->words_trace,
+                                                      cudaMemcpyHostToDevice, copy_stream) != cudaSuccess)
+                    return B200_ECUDA;
+            }
+            if (cudaEventRecord(u->copied, copy_stream) != cudaSuccess) return B200_ECUDA;
+            if (cudaStreamWaitEvent(s, u->copied, 0) != cudaSuccess) return B200_ECUDA;
+            if (last_done && cudaStreamWaitEvent(s, last_done, 0) != cudaSuccess) return B200_ECUDA;
+            if (cudaEventRecord(u->started, s) != cudaSuccess) return B200_ECUDA;
             std::vector<batch::Inst> in;
             for (Request *r : u->reqs)
                 in.push_back(batch::Inst{r->d_trace, r->d_scratch, r->d_lde, r->d_tree, r->nBits, r->nBitsExt,
@@ -305,6 +343,23 @@ class Server {
         if (!(u->done = take_event()) || cudaEventRecord(u->done, s) != cudaSuccess) return B200_ECUDA;
         last_done = u->done;
         return B200_OK;
+    }
+
+    void release_events(Unit *u)
+    {
+        for (cudaEvent_t e : {u->issued, u->copied, u->started, u->done})
+            if (e) spare_events.push_back(e);
+        u->issued = u->copied = u->started = u->done = nullptr;
+    }
+
+    double since_t0(cudaEvent_t e) const
+    {
+        float ms = -1.0f;
+        if (!e || cudaEventElapsedTime(&ms, t0_event, e) != cudaSuccess) {
+            cudaGetLastError();
+            return -1.0;
+        }
+        return (double)ms;
     }
 
     int free_slot() const
@@ -366,7 +421,9 @@ class Server {
             u->stream = streams[slot];
             const double t = now_ms();
             for (Request *r : u->reqs) r->t_admit = t;
+            const double t_launch = now_ms();
             int rc = launch_unit(u);
+            launch_ms += now_ms() - t_launch;
             if (rc) {
                 for (Request *r : u->reqs) {
                     free_buffers(r, u->stream);
@@ -375,7 +432,7 @@ class Server {
                     r->t_done = now_ms();
                 }
                 if (u->d_table) cudaFreeAsync(u->d_table, u->stream);
-                if (u->done) spare_events.push_back(u->done);
+                release_events(u);
                 delete u->plan;
                 delete u;
                 continue;
@@ -397,9 +454,15 @@ class Server {
     void finish_unit(Unit *u, bool ok)
     {
         const double t = now_ms();
+        const double gi = ok ? since_t0(u->issued) : -1, gc = ok ? since_t0(u->copied) : -1,
+                     gs = ok ? since_t0(u->started) : -1, gd = ok ? since_t0(u->done) : -1;
         for (size_t i = 0; i < u->reqs.size(); i++) {
             Request *r = u->reqs[i];
             r->t_done = t;
+            r->g_issued = gi;
+            r->g_copied = gc;
+            r->g_start = gs;
+            r->g_done = gd;
             if (ok) {
                 const uint64_t *src = u->batched ? u->plan->h_roots + 4 * i : h_roots[u->slot];
                 memcpy(r->root, src, 32);
@@ -414,8 +477,8 @@ class Server {
             }
         }
         if (u->d_table) cudaFreeAsync(u->d_table, u->stream);
-        if (u->done) spare_events.push_back(u->done);
         if (last_done == u->done) last_done = nullptr;
+        release_events(u);
         slot_busy[u->slot] = 0;
         delete u->plan;
         delete u;
@@ -525,14 +588,16 @@ extern "C" int b200_server_configure(void *srv, int batching, uint64_t small_ele
 }
 
 // counters, in this order: plain units, batched units, requests in batched units, pool trims (an
-// admission that did not fit the pool's cached blocks), times a waiting request was passed
+// admission that did not fit the pool's cached blocks), times a waiting request was passed,
+// microseconds the worker spent enqueueing units
 extern "C" int b200_server_stats(void *srv, uint64_t *out, uint64_t n)
 {
     auto *s = (serve::Server *)srv;
     if (!s || (n && !out)) return set_err(B200_EINVAL, "null argument");
     std::lock_guard<std::mutex> lk(s->mu);
-    const uint64_t v[5] = {s->units_plain, s->units_batched, s->batched_requests, s->pool_trims, s->overtakes};
-    for (uint64_t i = 0; i < n && i < 5; i++) out[i] = v[i];
+    const uint64_t v[6] = {s->units_plain, s->units_batched, s->batched_requests, s->pool_trims, s->overtakes,
+                           (uint64_t)(s->launch_ms * 1e3)};
+    for (uint64_t i = 0; i < n && i < 6; i++) out[i] = v[i];
     return B200_OK;
 }
 
@@ -548,6 +613,23 @@ extern "C" int b200_server_request_times(void *srv, int64_t id, double *times3)
     times3[0] = r->t_submit - s->t_start;
     times3[1] = r->t_admit ? r->t_admit - s->t_start : -1;
     times3[2] = r->t_done ? r->t_done - s->t_start : -1;
+    return B200_OK;
+}
+
+// device timeline of a completed request's unit in ms since the server was created (device clock):
+// copies issued, host-to-device copies done, kernels started, kernels done; -1 where not (yet) known
+extern "C" int b200_server_request_gpu_times(void *srv, int64_t id, double *times4)
+{
+    auto *s = (serve::Server *)srv;
+    if (!s || !times4) return set_err(B200_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return set_err(B200_EINVAL, "unknown request id");
+    const serve::Request *r = it->second;
+    times4[0] = r->g_issued;
+    times4[1] = r->g_copied;
+    times4[2] = r->g_start;
+    times4[3] = r->g_done;
     return B200_OK;
 }
 

@@ -139,10 +139,13 @@ def test_one_shot_batch_entry(pkg, torch_cuda):
 def test_server_alone_equals_in_the_mix(pkg, torch_cuda, mode, small):
     """Each request's root is the same served alone and served among overlapping requests: with
     continuous batching (small requests admitted together share one batched unit; with the lower
-    threshold the larger ones run as plain units beside them) and in FIFO mode."""
+    threshold the larger ones run as plain units beside them) and in FIFO mode.  Plain units of
+    2^16 rows and >= 128 columns cross in column blocks extended as they land, the first request
+    (on an idle device) with its rows hashed in chunks meanwhile."""
     lib = pkg.load()
+    # the last two cross in column blocks when they run as plain units (2^16 rows, >= 128 columns)
     shapes = [(12, 13, 40, 4), (14, 15, 9, 4), (10, 12, 100, 3), (15, 16, 30, 4), (9, 10, 5, 2), (13, 14, 64, 4),
-              (16, 17, 24, 4)]
+              (16, 17, 24, 4), (16, 17, 200, 4), (16, 18, 130, 3)]
     traces = [oracle.random_field((1 << nb, nc), 42 + i) for i, (nb, nbe, nc, ar) in enumerate(shapes)]
     alone = [pkg.commit_host(tr, nbe, ar)[0] for tr, (nb, nbe, nc, ar) in zip(traces, shapes)]
     srv = lib.b200_server_new(0, 8 << 30, 4)
@@ -159,16 +162,29 @@ def test_server_alone_equals_in_the_mix(pkg, torch_cuda, mode, small):
                 outs.append(out)
         assert lib.b200_server_wait_all(srv, 60000) == 0, lib.b200_last_error()
         lat = ctypes.c_double()
+        g = (ctypes.c_double * 4)()
+        spans = set()
         for (i, rid), out in zip(ids, outs):
             assert lib.b200_server_status(srv, rid, ctypes.byref(lat)) == 1
             assert lat.value > 0
             assert (out == alone[i]).all(), i
+            # device timeline: issued <= kernels started <= kernels done, and the copies done after
+            # issue and before the kernels end (a plain unit's kernels start on its first column
+            # block, so they may start before the last block has landed)
+            assert lib.b200_server_request_gpu_times(srv, rid, g) == 0
+            eps = 1e-3
+            assert 0 <= g[0] <= g[2] + eps and g[2] <= g[3] + eps, list(g)
+            assert g[0] <= g[1] + eps and g[1] <= g[3] + eps, list(g)
+            spans.add((g[2], g[3]))
             # the LDE stays resident until release
             d_lde = ctypes.c_void_p()
             d_tree = ctypes.c_void_p()
             assert lib.b200_server_buffers(srv, rid, ctypes.byref(d_lde), ctypes.byref(d_tree)) == 0
             assert d_lde.value and d_tree.value
             assert lib.b200_server_release(srv, rid) == 0
+        # the units' kernels run one after another, in admission order
+        spans = sorted(spans)
+        assert all(nxt[0] >= prev[1] - 1e-3 for prev, nxt in zip(spans, spans[1:])), spans
         # an oversized request is refused, not queued forever
         assert lib.b200_server_submit(srv, traces[0].ctypes.data, 24, 26, 64, 4, None) == pkg.B200_EBUSY
         st = (ctypes.c_uint64 * 5)()
