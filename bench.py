@@ -681,8 +681,8 @@ def serve_stream(lib, pool, hosts, arrivals, picks, mode, budget_gb, slots, time
                 raise RuntimeError("served stream did not finish within %.0f s" % timeout_s)
             time.sleep(0.001)
         wall = time.perf_counter() - t0
-        st = (ctypes.c_uint64 * 6)()
-        lib.b200_server_stats(srv, st, 6)
+        st = (ctypes.c_uint64 * 7)()
+        lib.b200_server_stats(srv, st, 7)
         times, g = (ctypes.c_double * 3)(), (ctypes.c_double * 4)()
         waits, service, units = [], [], set()
         for rid in ids:
@@ -691,8 +691,9 @@ def serve_stream(lib, pool, hosts, arrivals, picks, mode, budget_gb, slots, time
             service.append(times[2] - times[1])
             lib.b200_server_request_gpu_times(srv, rid, g)
             units.add(tuple(g))  # a batched unit's requests share its timeline
-        stats = {"plain_units": st[0], "batched_units": st[1], "batched_requests": st[2], "pool_trims": st[3],
+        stats = {"plain_units": st[0], "batched_units": st[1], "batched_requests": st[2], "waited_for_block": st[3],
                  "overtakes": st[4], "host_enqueue_ms": round(st[5] / 1e3, 1),
+                 "host_alloc_ms": round(st[6] / 1e3, 1),
                  "mean_wait_to_admission_ms": round(float(np.mean(waits)), 2),
                  "mean_admission_to_done_ms": round(float(np.mean(service)), 2), **gpu_timeline(units)}
     finally:
@@ -708,9 +709,15 @@ def serve_rates(rates, duration, n_c3, budget_gb, slots, timeout_s, serial=True,
     (batching, FIFO, FIFO, batching, ...) so that neither always runs first; the latencies reported
     are the means over a mode's runs, each run kept under "runs".  Near saturation a few percent of
     throughput moves the queueing delay a lot, so single runs of the two modes compare poorly."""
+    import torch
+
     pkg = load_package()
     pkg.init(0)
     lib = pkg.load()
+    # the server reserves its budget on the device when created: keep it within what is free
+    torch.cuda.empty_cache()
+    free_gb = torch.cuda.mem_get_info(0)[0] / 2**30
+    budget_gb = min(budget_gb, free_gb - 4.0)
     pool, hosts = serve_pool(lib, n_c3)
     # untimed warm-up: every shape once through each mode (module loading, first device allocations)
     for mode in (1, 0):
@@ -753,6 +760,7 @@ def serve_rates(rates, duration, n_c3, budget_gb, slots, timeout_s, serial=True,
             if rk and not all((x == rk[0]).all() for x in rk):
                 raise RuntimeError("served roots differ for one input")
         entry["roots_consistent"] = True
+        entry["device_budget_gib"] = round(budget_gb, 1)
         out.append(entry)
     del hosts
     return out, len(pool)

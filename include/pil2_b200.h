@@ -273,13 +273,16 @@ int b200_commit_batch_device(const B200BatchInstance *inst, uint64_t n, uint64_t
 
 /* ---- Commit server (continuous batching) ------------------------------------------------
  * Requests (host row-major traces; pinned memory lets the copies overlap) are admitted as soon
- * as one of `slots` slots is free and the request's device buffers fit in `budget_bytes` (the
- * server's own memory pool); an admitted unit's host-to-device copy overlaps the kernels of the
- * units ahead of it, and the units' kernels run in admission order.  The small requests waiting
+ * as one of `slots` slots is free and the request's device buffers fit in `budget_bytes`, which
+ * b200_server_new reserves on the device at once (one allocation, carved per request on the host;
+ * NULL with B200_ENOMEM when it cannot be reserved); an admitted unit's host-to-device copy
+ * overlaps the kernels of the units ahead of it (a large trace crosses in column blocks, each
+ * extended as it lands), and the units' kernels run in admission order.  The small requests waiting
  * together (LDE of at most small_elems elements) are admitted as one batched unit (one
  * b200_batch_plan over all of them) and may pass waiting large requests, each of which is passed
  * at most four times.  The LDE and tree of a finished request stay on the device
- * (b200_server_buffers, for query reads) until b200_server_release.  The reference's stream pool
+ * (b200_server_buffers, for query reads) until b200_server_release; release them only after the
+ * caller's own work on those buffers has completed, since the next admission may reuse them.  The reference's stream pool
  * + selectStream + get_stream_proofs loop (starks_api.cu:1138-1170, 2665-...) is the
  * one-request-per-stream counterpart. */
 void *b200_server_new(int device, uint64_t budget_bytes, uint32_t slots);
@@ -287,9 +290,10 @@ void *b200_server_new(int device, uint64_t budget_bytes, uint32_t slots);
  * arrival order; the comparison point); small_elems (default 2^26) and max_batch (requests per
  * batched unit, default 64). */
 int b200_server_configure(void *srv, int batching, uint64_t small_elems, uint32_t max_batch);
-/* counters into out[0..n): plain units, batched units, requests in batched units, pool trims (an
- * admission that did not fit the pool's cached blocks), times a waiting request was passed,
- * microseconds the worker spent enqueueing units (allocations, copies, launches) */
+/* counters into out[0..n): plain units, batched units, requests in batched units, requests that
+ * fit the budget but once found no contiguous block of it free (and waited), times a waiting
+ * request was passed, microseconds the worker spent enqueueing units (allocations, copies,
+ * launches), microseconds of that in allocations */
 int b200_server_stats(void *srv, uint64_t *out, uint64_t n);
 /* submission, admission and completion time of a request in ms since the server was created
  * (times3[1], times3[2] = -1 until reached) */

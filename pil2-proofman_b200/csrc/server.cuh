@@ -21,10 +21,13 @@
 // admitted ahead of the queue head — but a request is overtaken at most `max_overtakes` times, so
 // none waits forever.  Completion is observed through an event per unit; the LDE and the tree of
 // every request stay resident on the device (for later query reads) until the caller releases the
-// request.  Device buffers come from the server's own stream-ordered memory pool
-// (cudaMemPoolCreate), which keeps freed blocks cached for the next admissions without changing
-// the device's default pool.  No call blocks on the GPU except b200_server_wait_all, whose wait is
-// bounded by its timeout, and the pool trim of an admission that does not fit the cached blocks.
+// request.  Device buffers come from one device allocation of the budget, made when the server is
+// created and carved by a host-side best-fit arena: a request takes two blocks, [trace | scratch]
+// returned when its unit completes and [LDE | tree] returned when the caller releases it.  Carving
+// is host bookkeeping of a few microseconds; a stream-ordered memory pool measured 25-30 ms per
+// allocation for this size mix, which at 20 requests/s left the GPU idle ~20 % of the time while
+// requests waited.  No call blocks on the GPU except b200_server_wait_all, whose wait is bounded
+// by its timeout.
 //
 // Mode 0 (b200_server_configure) is the plain FIFO: every request a plain unit in arrival order;
 // kept as the comparison point.
@@ -32,6 +35,8 @@
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <iterator>
+#include <map>
 #include <unordered_map>
 
 #include "batch.cuh"
@@ -61,6 +66,7 @@ struct Request {
     // previous unit finished), kernels done
     double g_issued = -1, g_copied = -1, g_start = -1, g_done = -1;
     uint32_t overtaken = 0;  // times a batch of smaller requests was admitted ahead of it
+    bool waited_for_block = false;  // once found no contiguous block of the budget free
     std::string err;  // reason of a failed request (reported to the caller by status())
     uint64_t bytes() const { return 8 * (2 * words_trace + words_lde + words_tree); }
     uint64_t elems() const { return (uint64_t)nCols << nBitsExt; }
@@ -75,10 +81,69 @@ struct Unit {
     cudaEvent_t done = nullptr;
     cudaEvent_t issued = nullptr, copied = nullptr, started = nullptr;  // timeline (timing enabled, like done)
     batch::Plan *plan = nullptr;
-    unsigned char *d_table = nullptr;  // batched: the plan's device tables (from the pool)
 };
 
 constexpr size_t STAGING_BYTES = 1u << 20;  // per slot: a batched unit's tables and roots (pinned)
+
+// Best-fit arena over one device allocation; blocks are 256-byte aligned.  Host bookkeeping only:
+// the caller returns a block once no queued or running work uses it.
+class Arena {
+  public:
+    uint64_t *base = nullptr;
+    uint64_t words = 0;
+
+    int init(uint64_t bytes)
+    {
+        words = (bytes + 255) / 256 * 32;
+        if (cudaMalloc((void **)&base, 8 * words) != cudaSuccess) {
+            cudaGetLastError();
+            base = nullptr;
+            words = 0;
+            return set_err(B200_ENOMEM, "commit server: the device-memory budget could not be reserved");
+        }
+        free_[0] = words;
+        return B200_OK;
+    }
+    ~Arena()
+    {
+        if (base) cudaFree(base);
+    }
+    static uint64_t round(uint64_t w) { return (w + 31) / 32 * 32; }
+    uint64_t *take(uint64_t w)
+    {
+        w = round(w ? w : 1);
+        auto best = free_.end();
+        for (auto it = free_.begin(); it != free_.end(); ++it)
+            if (it->second >= w && (best == free_.end() || it->second < best->second)) best = it;
+        if (best == free_.end()) return nullptr;
+        const uint64_t off = best->first, len = best->second;
+        free_.erase(best);
+        if (len > w) free_[off + w] = len - w;
+        return base + off;
+    }
+    void give(uint64_t *p, uint64_t w)
+    {
+        if (!p) return;
+        w = round(w ? w : 1);
+        uint64_t off = (uint64_t)(p - base);
+        auto next = free_.lower_bound(off);
+        if (next != free_.end() && off + w == next->first) {  // merge with the block after
+            w += next->second;
+            next = free_.erase(next);
+        }
+        if (next != free_.begin()) {  // merge with the block before
+            auto prev = std::prev(next);
+            if (prev->first + prev->second == off) {
+                prev->second += w;
+                return;
+            }
+        }
+        free_[off] = w;
+    }
+
+  private:
+    std::map<uint64_t, uint64_t> free_;  // offset -> length (words), coalesced
+};
 
 class Server {
   public:
@@ -92,6 +157,7 @@ class Server {
     cudaStream_t copy_stream = nullptr;                // every unit's host-to-device copies, in admission order
     std::vector<std::vector<cudaEvent_t>> block_events;  // [slot] one per column block of a plain unit
     std::vector<unsigned char *> staging;            // [slot] pinned
+    std::vector<unsigned char *> d_tables;           // [slot] device copy of a batched unit's tables
     std::vector<uint64_t *> h_roots;                 // [slot] pinned, plain units' root
     std::vector<int> slot_busy;
     std::mutex mu;
@@ -102,13 +168,15 @@ class Server {
     int64_t next_id = 1;
     bool stop = false, configured = false;
     std::thread worker;
-    cudaMemPool_t pool = nullptr;
+    Arena arena;
     cudaEvent_t last_done = nullptr;  // completion of the most recently admitted unit
     cudaEvent_t t0_event = nullptr;   // device-time origin of the request timelines
     std::vector<cudaEvent_t> spare_events;
     int family = 2;                   // hash family of this server's commits (fixed at creation)
-    uint64_t units_plain = 0, units_batched = 0, batched_requests = 0, pool_trims = 0, overtakes = 0;
-    double launch_ms = 0;  // host time spent enqueueing units (allocations, copies, kernel launches)
+    uint64_t units_plain = 0, units_batched = 0, batched_requests = 0, overtakes = 0;
+    uint64_t deferred = 0;  // requests that fit the budget but once found no contiguous block, and waited
+    double launch_ms = 0;   // host time spent enqueueing units (allocations, copies, kernel launches)
+    double alloc_ms = 0;    // the part of it spent in the allocations
     double t_start = 0;
 
     int start(int dev, uint64_t budget_bytes, uint32_t slots)
@@ -121,13 +189,7 @@ class Server {
         if (rc) return rc;
         if ((rc = batch_kernel_attrs())) return rc;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaMemPoolProps props{};
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = dev;
-        CK(cudaMemPoolCreate(&pool, &props), "server memory pool");
-        uint64_t keep = UINT64_MAX;  // keep freed blocks cached in this pool
-        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "mem pool threshold");
+        if ((rc = arena.init(budget + (1u << 20)))) return rc;  // slack for the blocks' alignment
         for (uint32_t i = 0; i < slots; i++) {
             cudaStream_t s;
             CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
@@ -137,6 +199,9 @@ class Server {
             uint64_t *hr = nullptr;
             CK(cudaMallocHost((void **)&st, STAGING_BYTES), "pinned staging");
             staging.push_back(st);
+            unsigned char *dt = nullptr;
+            CK(cudaMalloc((void **)&dt, STAGING_BYTES), "batched tables");
+            d_tables.push_back(dt);
             CK(cudaMallocHost((void **)&hr, 32), "pinned root");
             h_roots.push_back(hr);
             slot_busy.push_back(0);
@@ -162,7 +227,7 @@ class Server {
         for (Unit *u : running) finish_unit(u, cudaEventQuery(u->done) == cudaSuccess);
         for (auto &kv : all) {
             Request *r = kv.second;
-            free_buffers(r, nullptr);
+            free_buffers(r);
             delete r;
         }
         cudaDeviceSynchronize();
@@ -171,21 +236,25 @@ class Server {
         for (auto &v : block_events)
             for (cudaEvent_t e : v) cudaEventDestroy(e);
         for (unsigned char *p : staging) cudaFreeHost(p);
+        for (unsigned char *p : d_tables) cudaFree(p);
         for (uint64_t *p : h_roots) cudaFreeHost(p);
         for (cudaEvent_t e : spare_events) cudaEventDestroy(e);
         if (t0_event) cudaEventDestroy(t0_event);
-        if (pool) cudaMemPoolDestroy(pool);
     }
 
-    // the two blocks of a request (d_scratch and d_tree point into them)
-    void free_buffers(Request *r, cudaStream_t s)
+    // [trace | scratch] back to the arena (the unit's work on it is complete)
+    void free_trace(Request *r)
     {
-        for (uint64_t **p : {&r->d_trace, &r->d_lde})
-            if (*p) {
-                cudaFreeAsync(*p, s);
-                *p = nullptr;
-            }
-        r->d_scratch = r->d_tree = nullptr;
+        arena.give(r->d_trace, 2 * r->words_trace);
+        r->d_trace = r->d_scratch = nullptr;
+    }
+
+    // both blocks of a request (d_scratch and d_tree point into them)
+    void free_buffers(Request *r)
+    {
+        free_trace(r);
+        arena.give(r->d_lde, r->words_lde + r->words_tree);
+        r->d_lde = r->d_tree = nullptr;
     }
 
     int64_t submit(const uint64_t *trace, uint32_t nBits, uint32_t nBitsExt, uint32_t nCols, uint32_t arity,
@@ -217,48 +286,22 @@ class Server {
         return r->id;
     }
 
-    cudaError_t pool_alloc(uint64_t **p, uint64_t words, cudaStream_t s)
+    // A request's two blocks, or none (and the admission waits for blocks to come back)
+    bool alloc_request(Request *r)
     {
-        return cudaMallocFromPoolAsync((void **)p, 8 * (words ? words : 1), pool, s);
-    }
-
-    // A request's buffers as two pool blocks, or none: [trace | scratch], released behind its
-    // kernels, and [LDE | tree], kept until the request is released (fewer, larger blocks keep the
-    // pool's cache less fragmented than one block per buffer).
-    bool alloc_request(Request *r, cudaStream_t s)
-    {
-        const uint64_t w1 = 2 * r->words_trace, w2 = r->words_lde + r->words_tree;
-        if (pool_alloc(&r->d_trace, w1, s) == cudaSuccess && pool_alloc(&r->d_lde, w2, s) == cudaSuccess) {
-            r->d_scratch = r->d_trace + r->words_trace;
-            r->d_tree = r->d_lde + r->words_lde;
-            return true;
+        const double t = now_ms();
+        r->d_trace = arena.take(2 * r->words_trace);
+        r->d_lde = r->d_trace ? arena.take(r->words_lde + r->words_tree) : nullptr;
+        alloc_ms += now_ms() - t;
+        if (!r->d_lde) {
+            free_buffers(r);
+            if (!r->waited_for_block) deferred++;
+            r->waited_for_block = true;
+            return false;
         }
-        cudaGetLastError();
-        free_buffers(r, s);
-        return false;
-    }
-
-    // Buffers of every request of a unit; when the cached blocks do not fit, the pool is trimmed
-    // (after the running units' frees have executed) and the allocation retried once.
-    bool alloc_unit(Unit *u)
-    {
-        for (int attempt = 0; attempt < 2; attempt++) {
-            bool ok = true;
-            for (Request *r : u->reqs)
-                if (!alloc_request(r, u->stream)) {
-                    ok = false;
-                    break;
-                }
-            if (ok) return true;
-            for (Request *r : u->reqs) free_buffers(r, u->stream);
-            if (attempt == 0) {
-                for (cudaStream_t t : streams) cudaStreamSynchronize(t);
-                cudaMemPoolTrimTo(pool, 0);
-                pool_trims++;
-                cudaGetLastError();
-            }
-        }
-        return false;
+        r->d_scratch = r->d_trace + r->words_trace;
+        r->d_tree = r->d_lde + r->words_lde;
+        return true;
     }
 
     cudaEvent_t take_event()
@@ -277,10 +320,6 @@ class Server {
     int launch_unit(Unit *u)
     {
         cudaStream_t s = u->stream;
-        if (!alloc_unit(u)) {
-            for (Request *r : u->reqs) r->err = "device buffers for the request could not be allocated";
-            return B200_ENOMEM;
-        }
         if (!(u->issued = take_event()) || cudaEventRecord(u->issued, s) != cudaSuccess) return B200_ECUDA;
         if (!(u->copied = take_event()) || !(u->started = take_event())) return B200_ECUDA;
         if (!u->batched) {
@@ -325,20 +364,12 @@ class Server {
                 return set_err(B200_EINVAL, "batched unit: descriptor tables above the staging size");
             unsigned char *st = staging[u->slot];
             memcpy(st, u->plan->table.data(), u->plan->table.size());
-            if (cudaMallocFromPoolAsync((void **)&u->d_table, tbytes, pool, s) != cudaSuccess) {
-                cudaGetLastError();
-                return B200_ENOMEM;
-            }
-            if (cudaMemcpyAsync(u->d_table, st, u->plan->table.size(), cudaMemcpyHostToDevice, s) != cudaSuccess)
+            if (cudaMemcpyAsync(d_tables[u->slot], st, u->plan->table.size(), cudaMemcpyHostToDevice, s) !=
+                cudaSuccess)
                 return B200_ECUDA;
-            u->plan->d_table = u->d_table;
+            u->plan->d_table = d_tables[u->slot];
             u->plan->h_roots = (uint64_t *)(st + tbytes);
             if (u->plan->enqueue(s) != cudaSuccess) return B200_ECUDA;
-        }
-        // the trace copy and the scratch are not needed once the commit has run
-        for (Request *r : u->reqs) {
-            cudaFreeAsync(r->d_trace, s);
-            r->d_trace = r->d_scratch = nullptr;
         }
         if (!(u->done = take_event()) || cudaEventRecord(u->done, s) != cudaSuccess) return B200_ECUDA;
         last_done = u->done;
@@ -372,7 +403,8 @@ class Server {
     // One admission round (caller holds mu): while a slot is free, the next unit holds the waiting
     // small requests (in arrival order, up to max_batch; a batch when there are several), passing
     // the large requests between them unless one of those has been overtaken max_overtakes times;
-    // with no small request waiting, the queue head.  Stops at the first unit the budget cannot hold.
+    // with no small request waiting, the queue head.  Stops at the first unit the budget cannot hold
+    // or the arena has no blocks for (the next completion or release retries).
     void admit()
     {
         while (!queue.empty()) {
@@ -386,7 +418,7 @@ class Server {
                 for (size_t i = 0; i < queue.size() && small.size() < max_batch; i++) {
                     Request *r = queue[i];
                     if (r->elems() <= small_elems) {
-                        if (used + add + r->bytes() > budget) break;
+                        if (used + add + r->bytes() > budget || !alloc_request(r)) break;
                         small.push_back(i);
                         add += r->bytes();
                     } else if (r->overtaken >= max_overtakes) {
@@ -409,7 +441,7 @@ class Server {
             }
             if (u->reqs.empty()) {
                 Request *head = queue.front();
-                if (used + head->bytes() > budget) {
+                if (used + head->bytes() > budget || !alloc_request(head)) {
                     delete u;
                     return;
                 }
@@ -425,13 +457,16 @@ class Server {
             int rc = launch_unit(u);
             launch_ms += now_ms() - t_launch;
             if (rc) {
+                // whatever was enqueued before the failure finishes before the blocks are reused
+                cudaStreamSynchronize(copy_stream);
+                cudaStreamSynchronize(u->stream);
+                cudaGetLastError();
                 for (Request *r : u->reqs) {
-                    free_buffers(r, u->stream);
+                    free_buffers(r);
                     if (r->err.empty()) r->err = "request failed on the device (CUDA error)";
                     r->status = rc;
                     r->t_done = now_ms();
                 }
-                if (u->d_table) cudaFreeAsync(u->d_table, u->stream);
                 release_events(u);
                 delete u->plan;
                 delete u;
@@ -468,15 +503,15 @@ class Server {
                 memcpy(r->root, src, 32);
                 if (r->root_out) memcpy(r->root_out, r->root, 32);
                 r->status = 2;
-                used -= 8 * 2 * r->words_trace;  // trace + scratch were freed behind the kernels
+                free_trace(r);  // the unit's kernels are done with the trace and the scratch
+                used -= 8 * 2 * r->words_trace;
             } else {
                 r->status = B200_ECUDA;
                 r->err = "request failed on the device (CUDA error)";
-                free_buffers(r, u->stream);
+                free_buffers(r);
                 used -= r->bytes();
             }
         }
-        if (u->d_table) cudaFreeAsync(u->d_table, u->stream);
         if (last_done == u->done) last_done = nullptr;
         release_events(u);
         slot_busy[u->slot] = 0;
@@ -546,7 +581,7 @@ class Server {
         if (r->status != 2 && r->status >= 0) return set_err(B200_EBUSY, "request still in flight");
         if (!r->released) {
             cudaSetDevice(device);
-            free_buffers(r, r->stream);
+            free_buffers(r);
             if (r->status == 2) used -= 8 * (r->words_lde + r->words_tree);
             r->released = true;
         }
@@ -587,17 +622,18 @@ extern "C" int b200_server_configure(void *srv, int batching, uint64_t small_ele
     return B200_OK;
 }
 
-// counters, in this order: plain units, batched units, requests in batched units, pool trims (an
-// admission that did not fit the pool's cached blocks), times a waiting request was passed,
-// microseconds the worker spent enqueueing units
+// counters, in this order: plain units, batched units, requests in batched units, requests that
+// fit the budget but once found no contiguous block in it (and waited for one), times a waiting request
+// was passed, microseconds the worker spent enqueueing units (allocations included), microseconds
+// of that in allocations
 extern "C" int b200_server_stats(void *srv, uint64_t *out, uint64_t n)
 {
     auto *s = (serve::Server *)srv;
     if (!s || (n && !out)) return set_err(B200_EINVAL, "null argument");
     std::lock_guard<std::mutex> lk(s->mu);
-    const uint64_t v[6] = {s->units_plain, s->units_batched, s->batched_requests, s->pool_trims, s->overtakes,
-                           (uint64_t)(s->launch_ms * 1e3)};
-    for (uint64_t i = 0; i < n && i < 6; i++) out[i] = v[i];
+    const uint64_t v[7] = {s->units_plain, s->units_batched, s->batched_requests, s->deferred, s->overtakes,
+                           (uint64_t)((s->launch_ms + s->alloc_ms) * 1e3), (uint64_t)(s->alloc_ms * 1e3)};
+    for (uint64_t i = 0; i < n && i < 7; i++) out[i] = v[i];
     return B200_OK;
 }
 
