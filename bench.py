@@ -203,6 +203,9 @@ def bench_config(args, wl, world):
                    "inputs (%.3f GB) fit in L2; no flush") % ((1 << nbits) * ncols * 8 / 1e9)}
 
 
+REF_MAX_STEPS = 6
+
+
 def time_reference_cpu(wl, reps, warmup, family=2):
     """The reference's CPU commit (NTT_Goldilocks::LDE + merkletree, compiled unmodified under oracle/_ref)
     of the full workload shape, with every host thread, as commit_witness_cpu runs it
@@ -246,7 +249,10 @@ def run_reference(args, wl):
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    val, sec, threads, sample, root = time_reference_cpu(wl, args.steps, args.warmup, args.hash_family)
+    # every step is one full commit of the workload (~15 s at C2 on 16 cores): at most
+    # REF_MAX_STEPS timed and one warm-up, so that the arm ends within a few minutes
+    reps, warm = max(1, min(args.steps, REF_MAX_STEPS)), min(args.warmup, 1)
+    val, sec, threads, sample, root = time_reference_cpu(wl, reps, warm, args.hash_family)
     fx = full_size_fixture(wl, args.hash_family)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(val, 6), "unit": UNIT, "n_gpus": args.gpus,
