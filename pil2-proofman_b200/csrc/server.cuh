@@ -35,10 +35,9 @@
 #include <chrono>
 #include <condition_variable>
 #include <deque>
-#include <iterator>
-#include <map>
 #include <unordered_map>
 
+#include "arena.h"
 #include "batch.cuh"
 
 namespace serve {
@@ -85,64 +84,39 @@ struct Unit {
 
 constexpr size_t STAGING_BYTES = 1u << 20;  // per slot: a batched unit's tables and roots (pinned)
 
-// Best-fit arena over one device allocation; blocks are 256-byte aligned.  Host bookkeeping only:
-// the caller returns a block once no queued or running work uses it.
+// The budget as one device allocation, carved by a BlockMap (arena.h).  Host bookkeeping only: the
+// caller returns a block once no queued or running work uses it.
 class Arena {
   public:
     uint64_t *base = nullptr;
-    uint64_t words = 0;
 
     int init(uint64_t bytes)
     {
-        words = (bytes + 255) / 256 * 32;
+        const uint64_t words = (bytes + 255) / 256 * BlockMap::UNIT;
         if (cudaMalloc((void **)&base, 8 * words) != cudaSuccess) {
             cudaGetLastError();
             base = nullptr;
-            words = 0;
             return set_err(B200_ENOMEM, "commit server: the device-memory budget could not be reserved");
         }
-        free_[0] = words;
+        map.reset(words);
         return B200_OK;
     }
     ~Arena()
     {
         if (base) cudaFree(base);
     }
-    static uint64_t round(uint64_t w) { return (w + 31) / 32 * 32; }
     uint64_t *take(uint64_t w)
     {
-        w = round(w ? w : 1);
-        auto best = free_.end();
-        for (auto it = free_.begin(); it != free_.end(); ++it)
-            if (it->second >= w && (best == free_.end() || it->second < best->second)) best = it;
-        if (best == free_.end()) return nullptr;
-        const uint64_t off = best->first, len = best->second;
-        free_.erase(best);
-        if (len > w) free_[off + w] = len - w;
-        return base + off;
+        const uint64_t off = map.take(w);
+        return off == BlockMap::NONE ? nullptr : base + off;
     }
     void give(uint64_t *p, uint64_t w)
     {
-        if (!p) return;
-        w = round(w ? w : 1);
-        uint64_t off = (uint64_t)(p - base);
-        auto next = free_.lower_bound(off);
-        if (next != free_.end() && off + w == next->first) {  // merge with the block after
-            w += next->second;
-            next = free_.erase(next);
-        }
-        if (next != free_.begin()) {  // merge with the block before
-            auto prev = std::prev(next);
-            if (prev->first + prev->second == off) {
-                prev->second += w;
-                return;
-            }
-        }
-        free_[off] = w;
+        if (p) map.give((uint64_t)(p - base), w);
     }
 
   private:
-    std::map<uint64_t, uint64_t> free_;  // offset -> length (words), coalesced
+    BlockMap map;
 };
 
 class Server {
