@@ -198,9 +198,11 @@ __device__ __forceinline__ uint64_t sub_c(uint64_t a, uint64_t b)
 }
 
 // x * 2^S mod p for 0 < S < 96 by shifts: x << S spans at most three 32-bit words placed at word
-// offset S/32; the 128-bit reduction folds it, and a word that lands at 2^128 is folded with
-// 2^128 = -2^32 (mod p).  Multiplication by the radix-16 roots of unity (powers of w_16 = 2^12)
-// costs three shifts and one reduction instead of four wide products.
+// offset S/32, folded with 2^64 = 2^32 - 1, 2^96 = -1 and 2^128 = -2^32 (mod p).  At offset 0 the
+// words are (u1:u0) + u2 * 2^64: one multiply-add and one carry fold; at offset 2 they are
+// u0 * 2^64 + (u2:u1) * 2^96: one product and one subtraction; offset 1 takes the general 128-bit
+// reduction.  Multiplication by the radix-16 roots of unity (powers of w_16 = 2^12) thus costs
+// three shifts and a short reduction instead of four wide products.
 template <int S>
 __device__ __forceinline__ uint64_t mul_pow2(uint64_t x)
 {
@@ -217,10 +219,27 @@ __device__ __forceinline__ uint64_t mul_pow2(uint64_t x)
         u1 = __funnelshift_l(x0, x1, T);
         u2 = x1 >> (32 - T);
     }
-    if (Q == 0) return reduce128(u0, u1, u2, 0u);
+    if (Q == 0) {
+        // (u1:u0) + u2 * 2^64 = (u1:u0) + u2 * (2^32 - 1): one carry at most, folded as 2^32 - 1
+        uint32_t z0, z1, c;
+        asm("mad.lo.cc.u32  %0, %5, 0xffffffff, %3;\n\t"
+            "madc.hi.cc.u32 %1, %5, 0xffffffff, %4;\n\t"
+            "addc.u32       %2, 0, 0;\n\t"
+            : "=r"(z0), "=r"(z1), "=r"(c)
+            : "r"(u0), "r"(u1), "r"(u2));
+        const uint32_t m = 0u - c;
+        asm("add.cc.u32 %0, %0, %2;\n\t"
+            "addc.u32   %1, %1, 0;\n\t"
+            : "+r"(z0), "+r"(z1)
+            : "r"(m));
+        return mk64(z0, z1);
+    }
     if (Q == 1) return reduce128(0u, u0, u1, u2);
-    const uint64_t y = reduce128(0u, 0u, u0, u1);
-    return sub_c(y, (uint64_t)u2 << 32);  // u2 < 2^T <= 2^31: u2 * 2^32 < p
+    // u0 * 2^64 + u1 * 2^96 + u2 * 2^128 = u0 * (2^32 - 1) - (u2 * 2^32 + u1), and u2 < 2^T <= 2^31
+    // keeps the subtrahend below p
+    uint64_t w;
+    asm("mul.wide.u32 %0, %1, 0xffffffff;" : "=l"(w) : "r"(u0));
+    return sub_c(w, mk64(u1, u2));
 }
 
 // x^7 = x^3 * x^4, the Poseidon2 S-box (poseidon2_goldilocks.hpp:147-155)
