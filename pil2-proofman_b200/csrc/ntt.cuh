@@ -102,7 +102,8 @@ __device__ __forceinline__ uint64_t mul_root16(uint64_t x, int idx)
 }
 
 // Forward radix-2^R DIT network.  The twiddled operand is made canonical, so the butterfly's add
-// and subtract each need one carry fold; the roots w_16^idx = 2^(12 idx) are shift multiplies.
+// and subtract each need one carry fold; the roots w_16^idx = 2^(12 idx) are shift multiplies,
+// and those of idx 6 and 7 (2^72, 2^84: a product and a subtraction) are canonical already.
 template <int R, bool INV>
 __device__ __forceinline__ void radix_dit(uint64_t (&v)[16])
 {
@@ -116,7 +117,7 @@ __device__ __forceinline__ void radix_dit(uint64_t (&v)[16])
             const int e = j & (h - 1);
             uint64_t x = v[j + h];
             if (e) x = mul_root16(x, e << (3 - u));
-            x = gl::canon(x);
+            if ((e << (3 - u)) < 6) x = gl::canon(x);
             const uint64_t y = v[j];
             v[j] = gl::add_c(y, x);
             v[j + h] = gl::sub_c(y, x);
@@ -125,7 +126,8 @@ __device__ __forceinline__ void radix_dit(uint64_t (&v)[16])
 }
 
 // Inverse radix-2^R DIF network.  w_16^-idx = -2^(96 - 12 idx), so a twiddled difference is
-// (x - y) * 2^(96 - 12 idx); the untwiddled ones use the canonical operand's single-fold forms.
+// (x - y) * 2^(96 - 12 idx), taken with y canonical; the untwiddled y - x with x canonical.  Either
+// way the sum and the difference need one carry fold each.
 template <int R, bool INV>
 __device__ __forceinline__ void radix_dif(uint64_t (&v)[16])
 {
@@ -137,12 +139,15 @@ __device__ __forceinline__ void radix_dif(uint64_t (&v)[16])
         for (int j = 0; j < (1 << R); j++) {
             if (j & h) continue;
             const int e = j & (h - 1);
-            const uint64_t y = v[j], x = gl::canon(v[j + h]);
-            v[j] = gl::add_c(y, x);
-            if (e)
-                v[j + h] = mul_root16(gl::sub(x, y), 8 - (e << (3 - u)));
-            else
+            if (e) {
+                const uint64_t y = gl::canon(v[j]), x = v[j + h];
+                v[j] = gl::add_c(x, y);
+                v[j + h] = mul_root16(gl::sub_c(x, y), 8 - (e << (3 - u)));
+            } else {
+                const uint64_t y = v[j], x = gl::canon(v[j + h]);
+                v[j] = gl::add_c(y, x);
                 v[j + h] = gl::sub_c(y, x);
+            }
         }
     }
 }
