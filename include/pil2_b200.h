@@ -282,9 +282,9 @@ int b200_commit_batch_device(const B200BatchInstance *inst, uint64_t n, uint64_t
  * b200_batch_plan over all of them) and may pass waiting large requests, each of which is passed
  * at most four times.  The LDE and tree of a finished request stay on the device
  * (b200_server_buffers, for query reads) until b200_server_release; release them only after the
- * caller's own work on those buffers has completed, since the next admission may reuse them.  The reference's stream pool
- * + selectStream + get_stream_proofs loop (starks_api.cu:1138-1170, 2665-...) is the
- * one-request-per-stream counterpart. */
+ * caller's own work on those buffers has completed, since the next admission may reuse them.
+ * The reference's stream pool + selectStream + get_stream_proofs loop (starks_api.cu:1138-1170,
+ * 2665-...) is the one-request-per-stream counterpart. */
 void *b200_server_new(int device, uint64_t budget_bytes, uint32_t slots);
 /* Before the first submit: batching 1 (default) as above, 0 = FIFO (every request a plain unit in
  * arrival order; the comparison point); small_elems (default 2^26) and max_batch (requests per
